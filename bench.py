@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark of the exact L_d solver (plain Gray-code enumeration).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config 2] [--impl ours|reference]
+
+One step is one complete exact solve of the workload (configuration 2 by
+default: the 40x40 marginal Bell expression with flags `y m`, reduced to
+34x37, 2^33 labelings).  `value` is labelings/s over K device-timed steps
+(CUDA events on the solver's stream, L2 flushed between steps, inputs
+resident); `e2e` is the same metric through the public API from host
+buffers (upload, solve, 16-byte result read, strategy report).  With N > 1
+(torchrun) every rank enumerates its shard of the same solve and the ranks
+combine the 16-byte (value, Gray index) candidate with two NCCL all-reduces;
+the time is the max over ranks.
+
+`--impl reference` times the reference's own OpenMP solver (oracle/_ref,
+built from the reference sources) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "l-norms_bruteforce_b200"
+REF_BIN = ROOT / "oracle" / "_ref" / "L_OpenMP"
+
+
+def load_package():
+    if "lnorms_b200" in sys.modules:
+        return sys.modules["lnorms_b200"]
+    spec = importlib.util.spec_from_file_location("lnorms_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["lnorms_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def instance(cfg: int):
+    load_package()
+    import lnorms_b200.workloads as W
+    return {1: W.config1, 2: W.config2, 3: W.config3, 5: W.config5}[cfg]()
+
+
+def ops_per_labeling(d: int, cols: int) -> int:
+    """Algorithmic integer work per labeling: update + |.| + accumulate per
+    column (3m) for L_1/LM; two changed message vectors (6m) for d >= 2."""
+    return 3 * cols if d == 1 else 6 * cols
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = [ln.split(",") for ln in Path(self.file.name).read_text().splitlines() if ln.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        loaded = [s for s in sm if s >= 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU side
+def write_matrix(path: Path, a: np.ndarray) -> None:
+    path.write_text("".join(" ".join(str(int(v)) for v in row) + "\n" for row in a))
+
+
+def run_reference_binary(a: np.ndarray, tail: list[str], threads: int) -> tuple[float, str]:
+    with tempfile.TemporaryDirectory() as td:
+        write_matrix(Path(td) / "m.txt", a)
+        t0 = time.perf_counter()
+        p = subprocess.run([str(REF_BIN), str(threads), "m.txt", *tail], cwd=td, capture_output=True,
+                           text=True, timeout=900)
+        dt = time.perf_counter() - t0
+    if p.returncode != 0:
+        raise RuntimeError(f"reference solver failed: {p.stdout[-300:]} {p.stderr[-300:]}")
+    return dt, p.stdout
+
+
+def reference_sample(inst, ld, target_labelings: int):
+    """A bounded sample of the workload for the CPU: the reduced matrix with
+    free rows dropped until at most target_labelings remain (same columns,
+    so the per-labeling work is the workload's).  Returned as the file the
+    reference reads: marginal row first, flag `m` only."""
+    p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
+    info = p.info
+    red = p.reduced
+    rows = info["rows"]
+    base = 2 if info["d"] <= 2 else info["d"]
+    keep = rows
+    while keep > 1 and base ** (keep - 1) > target_labelings:
+        keep -= 1
+    sub = np.concatenate([red[: keep - 1], red[-1:]], axis=0)   # fixed row stays last
+    labelings = base ** (keep - 1)
+    if info["marginal"]:
+        a = np.concatenate([sub[-1:], sub[:-1]], axis=0)         # the reference swaps it back
+        tail = [str(info["d"]), "m"]
+    else:
+        a, tail = sub, [str(info["d"])]
+    return a, tail, labelings, f"reduced {inst.name} cut to {keep} rows x {info['cols']} cols"
+
+
+def cpu_baseline(inst, ld, target_seconds: float = 15.0) -> dict:
+    threads = os.cpu_count() or 1
+    # calibrate on a small sample, then size the timed sample to ~target_seconds
+    a, tail, n0, _ = reference_sample(inst, ld, 1 << 24)
+    if REF_BIN.exists():
+        t0, _ = run_reference_binary(a, tail, threads)
+        rate = n0 / max(t0, 1e-3)
+        a, tail, n, what = reference_sample(inst, ld, int(rate * target_seconds))
+        t, _ = run_reference_binary(a, tail, threads)
+        return {"value": n / t, "unit": "labelings/s", "cores": threads, "kind": "reference",
+                "sample": f"L_OpenMP.c built from the reference sources, {threads} threads, {what} "
+                          f"({n} labelings, {t:.2f} s)"}
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_ffi as O   # the oracle restatement, when the reference binary is absent
+    red_p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
+    info = red_p.info
+    red = red_p.reduced
+    t0 = time.perf_counter()
+    O.enumerate_max(red, info["d"], bool(info["marginal"]), 0, 1 << 24, threads)
+    rate = (1 << 24) / max(time.perf_counter() - t0, 1e-3)
+    n = int(min(O.total(info["rows"], info["d"]), rate * target_seconds))
+    t0 = time.perf_counter()
+    O.enumerate_max(red, info["d"], bool(info["marginal"]), 0, n, threads)
+    t = time.perf_counter() - t0
+    return {"value": n / t, "unit": "labelings/s", "cores": threads, "kind": "port",
+            "sample": f"oracle restatement, {threads} threads, first {n} labelings of {inst.name}"}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    ld = load_package()
+    inst = instance(args.config)
+    threads = os.cpu_count() or 1
+    if not REF_BIN.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/L_OpenMP was not built "
+                          "(make -C oracle needs the reference sources)"}))
+        return
+    # each step: a bounded sample of the workload sized to ~3 s on this host
+    a, tail, n0, _ = reference_sample(inst, ld, 1 << 24)
+    t0, _ = run_reference_binary(a, tail, threads)
+    rate = n0 / max(t0, 1e-3)
+    a, tail, n, what = reference_sample(inst, ld, int(rate * 3.0))
+    for _ in range(args.warmup):
+        run_reference_binary(a, tail, threads)
+    times = [run_reference_binary(a, tail, threads)[0] for _ in range(args.steps)]
+    total = sum(times)
+    value = n * args.steps / total
+    p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
+    info = p.info
+    sample = f"L_OpenMP.c built from the reference sources, {threads} threads, {what} ({n} labelings)"
+    line = {
+        "impl": "reference", "metric": "exact L_d labelings/s (plain enumeration)", "value": value,
+        "unit": "labelings/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator of the configuration)",
+        "config": {"workload": workload_name(inst, info), "rows": info["rows"], "cols": info["cols"],
+                   "d": info["d"], "marginal": bool(info["marginal"]), "labelings_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "labelings/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "labelings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def workload_name(inst, info) -> str:
+    return (f"{inst.name}: d={info['d_user']}{' marginal' if info['marginal_user'] else ''}, "
+            f"flag {inst.stat}, {info['rows_in']}x{info['cols_in']} -> {info['rows']}x{info['cols']}, "
+            f"{info['labelings']} labelings")
+
+
+# ---------------------------------------------------------------- GPU side
+class DeviceView:
+    """Zero-copy view of a device int64 pair (the plan's result slot)."""
+
+    def __init__(self, ptr: int):
+        self.__cuda_array_interface__ = {"shape": (2,), "typestr": "<i8", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ld = load_package()
+    inst = instance(args.config)
+    prob = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
+    info = prob.info
+    red = prob.reduced
+    d, marg = info["d"], bool(info["marginal"])
+    opts = ld.options(device=local, shard_index=rank, shard_count=world)
+    plan = ld.Plan(red, d, marg, opts)
+    lo, hi = plan.range
+    total_labelings = info["labelings"]
+    stream = torch.cuda.ExternalStream(plan.stream, device=torch.device("cuda", local))
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+
+    def step():
+        plan.launch()
+
+    def combine(val_idx):
+        # (value, index) -> global max value, smallest index attaining it
+        v = val_idx[0:1].clone()
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        idx = torch.where(val_idx[0:1] == v, val_idx[1:2],
+                          torch.full_like(val_idx[1:2], torch.iinfo(torch.int64).max))
+        dist.all_reduce(idx, op=dist.ReduceOp.MIN)
+        return v, idx
+
+    # the plan's result slot, viewed as a tensor for the cross-rank combine
+    res_view = None
+    if world > 1:
+        res_view = torch.as_tensor(DeviceView(plan.result_device_ptr), device="cuda")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+            if world > 1:
+                combine(res_view)
+                dist.barrier()
+        sol0 = plan.result()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            step()
+            if world > 1:
+                combine(res_view)
+            stops[i].record(stream)
+            flush.fill_(i & 0xFF)   # outside the timed events, same stream
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    my_total = sum(step_ms)
+    t = torch.tensor([my_total], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    sol = plan.result()
+    value = total_labelings * args.steps / (total_ms * 1e-3)
+
+    # end to end through the public API: host matrix in, value + strategy out
+    e2e_ms, h2d, d2h = [], 0, 0
+    for i in range(args.warmup + args.steps):
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
+        res = p.solve(ld.options(device=local, shard_index=rank, shard_count=world))
+        if world > 1:
+            pair = torch.tensor([res.value, res.gray_index], dtype=torch.int64, device="cuda")
+            v, idx = combine(pair)
+            res.value, res.gray_index = int(v.item()), int(idx.item())
+        p.report(res)
+        dt = (time.perf_counter() - t0) * 1e3
+        if i >= args.warmup:
+            e2e_ms.append(dt)
+            h2d, d2h = int(res.h2d_bytes), int(res.d2h_bytes)
+    e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = total_labelings * args.steps / (float(e2e_t.item()) * 1e-3)
+
+    if rank == 0:
+        kernel_ms = statistics.mean(step_ms)
+        opl = ops_per_labeling(d, info["cols"])
+        peak_ops, _ = ld.int32_peak(local)
+        achieved = opl * (hi - lo) / (kernel_ms * 1e-3)
+        line = {
+            "metric": "exact L_d labelings/s (plain enumeration)", "value": value, "unit": "labelings/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator of the configuration)",
+            "config": {"workload": workload_name(inst, info), "rows": info["rows"], "cols": info["cols"],
+                       "d": d, "marginal": marg, "labelings_per_step": total_labelings,
+                       "parallelism": f"gray-index shards x{world}" if world > 1 else "single GPU",
+                       "l2": "flushed between steps (512 MiB write outside the timed events)",
+                       "kernel": plan.describe(), "value": sol.value, "gray_index": sol.gray_index},
+            "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12,
+                         "unit": "Tops/s", "frac": achieved / peak_ops, "traffic": None,
+                         "note": f"{opl} algorithmic int32 ops per labeling ({'3m' if d == 1 else '6m'}, "
+                                 f"m={info['cols']}); peak = int32 add/xor microbenchmark measured in this run"},
+            "e2e": {"value": e2e_value, "unit": "labelings/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": statistics.mean(e2e_ms)},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(inst, ld)
+        assert sol0.value == sol.value and sol0.gray_index == sol.gray_index
+        print(json.dumps(line))
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 5])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,205 @@
+/*
+ * lnorms_b200.h -- C ABI of the B200-native exact L_d-norm solver.
+ *
+ * The reference (istvanmarton/L-norms_BruteForce) has no library API: its
+ * boundary is the executable `L_CUDA blocks threads matrix d [y|c|r] [m]`
+ * (L_CUDA.cu:361-439) built from the stage functions below.  This header
+ * exposes one entry point per stage, with plain pointers and sizes only, so
+ * a C host (the drop-in CLI in this package, a ctypes/cffi binding, or the
+ * reference's own main with its calc_Lnorm body replaced) can call it.
+ *
+ * Conventions
+ *  - Every function returns an ld_status (0 = LD_OK); nothing here exits or
+ *    prints.  ld_last_error() gives a one-line message for the calling
+ *    thread's last failure.
+ *  - The caller owns every host buffer it passes; the library owns device
+ *    memory (plans) and host objects it returns (problems), which the caller
+ *    releases with the matching *_destroy.
+ *  - A plan is single-threaded and runs on one CUDA stream (its own, or the
+ *    one given in ld_options).
+ *  - Matrix entries are int64 on the host.  The device path computes in
+ *    packed int8x4 / int16x2, int32 or int64 lanes, chosen from an exact
+ *    bound on every partial column sum, so results never overflow.
+ */
+#ifndef LNORMS_B200_H
+#define LNORMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    LD_OK = 0,
+    LD_ERR_ARG = 1,      /* invalid argument                                    */
+    LD_ERR_INPUT = 2,    /* malformed matrix text (no entries, ragged rows)     */
+    LD_ERR_LIMIT = 3,    /* too many rows for the Gray index, or > 4096 columns */
+    LD_ERR_CUDA = 4,     /* a CUDA runtime call failed                          */
+    LD_ERR_NODEV = 5,    /* no CUDA device (the library has no CPU fallback)    */
+    LD_ERR_IO = 6,       /* file could not be opened                            */
+    LD_ERR_TIMEOUT = 7,  /* a bounded device-side wait gave up                  */
+    LD_ERR_NOMEM = 8     /* host allocation failed                              */
+} ld_status;
+
+/* Result of one solve. */
+typedef struct {
+    int64_t value;         /* the L_d norm (LM for marginal problems)                */
+    uint64_t gray_index;   /* smallest Gray-code index attaining it (tie-break of
+                              L_CUDA.cu:80 strict '>' and :347 strict '<')          */
+    uint64_t labelings;    /* labelings the device evaluated or proved dominated    */
+    float kernel_ms;       /* device time of the solve's launches (CUDA events)     */
+    int32_t kernel_kind;   /* LD_KERNEL_* actually used                             */
+    int32_t lane_bits;     /* 8, 16, 32 or 64: arithmetic lane width used           */
+    uint64_t h2d_bytes;    /* host-to-device bytes this solve copied                */
+    uint64_t d2h_bytes;    /* device-to-host bytes this solve copied                */
+} ld_result;
+
+enum {
+    LD_KERNEL_NONE = 0,     /* zero matrix: nothing launched                     */
+    LD_KERNEL_TABLE = 1,    /* register kernel with a shared-memory table of the
+                               low rows' partial sums (d = 1, LM, 2, 3)           */
+    LD_KERNEL_WIDE = 2      /* column-parallel kernel (any d <= 10, <= 4096 cols,
+                               int32 or int64)                                    */
+};
+
+/* Tuning and placement knobs; ld_options_init() fills the defaults (0/-1 =
+ * automatic).  None of them changes the result. */
+typedef struct {
+    int32_t device;             /* CUDA device ordinal                            */
+    int32_t low_rows;           /* rows tabulated in shared memory (-1 auto)      */
+    int32_t threads_per_block;  /* 0 auto                                         */
+    int32_t blocks;             /* 0 auto (a multiple of the SM count)            */
+    int32_t tile;               /* prefixes walked together per thread (0 auto)   */
+    int32_t kernel;             /* 0 auto, else LD_KERNEL_TABLE / LD_KERNEL_WIDE  */
+    int32_t lane_bits;          /* 0 auto, else force 16 / 32 / 64 (>= needed)    */
+    int32_t shard_index;        /* this device's part of a solve split over       */
+    int32_t shard_count;        /* shard_count devices (0 or 1: the whole range)  */
+    int32_t reserved;
+    void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
+} ld_options;
+
+void ld_options_init(ld_options *opt);
+
+/* ---------------------------------------------------------------------- */
+/* Stage 1+2: read and preprocess.                                          */
+/* Replaces matrix_read (functions.h:40-79) and load_parameters             */
+/* (L_CUDA.cu:414-423: eliminate_zero_rows_cols functions.h:109-151,         */
+/* calc_reduce_matrix_rows :237-262, calc_reduce_matrix_cols :264-289,       */
+/* calc_reduce_matrix_cols_sign :193-235, delete_rows/cols :153-191,         */
+/* convert_mtx_to_vec :291-329) and the d reset of calc_Parameters           */
+/* (L_CUDA.cu:244-248).  `stat` is the preprocessing flag character          */
+/* (y/Y/r/R/c/C, anything else = none); `marginal` is honoured for d == 1    */
+/* only, as arguments_CUDA does (L_CUDA.cu:401).  The problem keeps the      */
+/* lines the reference prints on stdout; see ld_problem_log.                 */
+typedef struct ld_problem ld_problem;
+
+ld_status ld_problem_from_text(const char *text, size_t len, int32_t d, char stat,
+                               int32_t marginal, ld_problem **out);
+ld_status ld_problem_from_file(const char *path, int32_t d, char stat, int32_t marginal,
+                               ld_problem **out);
+/* Row-major rows x cols entries, as if read from a file. */
+ld_status ld_problem_from_matrix(const int64_t *a, int32_t rows, int32_t cols, int32_t d,
+                                 char stat, int32_t marginal, ld_problem **out);
+void ld_problem_destroy(ld_problem *p);
+
+/* Reduced shape: rows/cols after preprocessing (and transpose), effective d,
+ * marginal actually used, and the number of labelings (0 for a zero matrix;
+ * saturates at UINT64_MAX). */
+typedef struct {
+    int32_t rows_in, cols_in;
+    int32_t rows, cols;
+    int32_t d_user, d;
+    int32_t marginal_user, marginal;
+    int32_t transposed;
+    int32_t max_rows;          /* maximum length of the strategy vector          */
+    uint64_t labelings;
+} ld_problem_info;
+ld_status ld_problem_get_info(const ld_problem *p, ld_problem_info *info);
+/* The reduced matrix handed to the solver (mtx_as_vec of the reference):
+ * rows*cols int64, row-major, fixed (or marginal) row last. */
+ld_status ld_problem_reduced(const ld_problem *p, int64_t *out, size_t cap);
+/* Text the reference prints up to this stage (NUL-terminated, owned by p). */
+const char *ld_problem_log(const ld_problem *p);
+
+/* calc_Parameters' launch clamp and limit checks (L_CUDA.cu:267-278):
+ * appends "num_ofBlock ..." and "maximum length ..." to the log; returns
+ * LD_ERR_LIMIT (with the reference's message appended) when the reduced
+ * matrix exceeds its row or column limit. */
+ld_status ld_problem_check_launch(ld_problem *p, int32_t blocks, int32_t threads);
+
+/* ---------------------------------------------------------------------- */
+/* Stage 3: solve.  Replaces calc_Lnorm (L_CUDA.cu:281-359): device upload, */
+/* the L1/LM/L2/L3/Ln kernels (L_CUDA.cu:14-240) and the host argmax         */
+/* (L_CUDA.cu:341-348).  A zero matrix (rows == 0) yields value 0 without a  */
+/* launch, as main does (L_CUDA.cu:432).                                     */
+ld_status ld_problem_solve(ld_problem *p, const ld_options *opt, ld_result *res);
+
+/* Same, for an already reduced matrix (mtx_as_vec layout: row-major, the
+ * last row carries the fixed label / the marginal row).  d is the effective
+ * order.  `strategy` (may be NULL) receives rows-1 labels: 0/1 for d <= 2
+ * (1 = +1 for d == 1), 0..d-1 otherwise -- second->strategy of the
+ * reference. */
+ld_status ld_solve_reduced(const int64_t *mtx_as_vec, int32_t rows, int32_t cols, int32_t d,
+                           int32_t marginal, const ld_options *opt, ld_result *res,
+                           int32_t *strategy);
+
+/* Labels of rows 0..rows-2 for a Gray index (the BRGC word of L_CUDA.cu:61-63,
+ * the d-ary reflected word of L_CUDA.cu:204-206). */
+ld_status ld_gray_labels(uint64_t index, int32_t rows, int32_t d, int32_t *labels);
+
+/* ---------------------------------------------------------------------- */
+/* Stage 4: output.  Replaces print_results (functions.h:371-412): the       */
+/* "L%d is: %d" / "LM is: %d" line is appended to the log, and `strategy`    */
+/* (capacity cap) receives one label per ORIGINAL row (column if the matrix  */
+/* was transposed) in the file's encoding (+-1 for d == 1, 0..d-1 else);      */
+/* *count gets the number written; name gets "strategy_L%d.txt" or          */
+/* "strategy_LM.txt". */
+ld_status ld_problem_report(ld_problem *p, const ld_result *res, int32_t *strategy,
+                            int32_t cap, int32_t *count, char *name, size_t name_cap);
+
+/* ---------------------------------------------------------------------- */
+/* Plans: a device-resident reduced matrix for repeated solves (bench and   */
+/* batch callers).  Same arguments as ld_solve_reduced.                      */
+typedef struct ld_plan ld_plan;
+ld_status ld_plan_create(const int64_t *mtx_as_vec, int32_t rows, int32_t cols, int32_t d,
+                         int32_t marginal, const ld_options *opt, ld_plan **out);
+/* Enqueue one full solve on the plan's stream; no host synchronisation. */
+ld_status ld_plan_launch(ld_plan *plan);
+/* Wait for the last launch and read its 16-byte result. */
+ld_status ld_plan_result(ld_plan *plan, ld_result *res, int32_t *strategy);
+/* Gray-index range [lo, hi) the plan enumerates (its shard, or everything).
+ * Shards of the same problem on identical devices tile [0, labelings). */
+ld_status ld_plan_range(const ld_plan *plan, uint64_t *lo, uint64_t *hi);
+/* One-line description of the kernel configuration the plan chose. */
+ld_status ld_plan_describe(const ld_plan *plan, char *buf, size_t cap);
+/* The stream the plan launches on (cudaStream_t). */
+void *ld_plan_stream(const ld_plan *plan);
+/* Device address of the plan's 16-byte result {int64 value; uint64 index},
+ * valid after a launch completes on the plan's stream (for callers that
+ * combine shards on the device, e.g. with an NCCL all-reduce). */
+void *ld_plan_result_device(const ld_plan *plan);
+void ld_plan_destroy(ld_plan *plan);
+
+/* ---------------------------------------------------------------------- */
+/* The drop-in executable: `blocks threads matrix d [y|c|r] [m]`, same      */
+/* argument checks, stdout lines and strategy file as L_CUDA's main and     */
+/* arguments_CUDA (L_CUDA.cu:361-439).  Returns the process exit status.    */
+int ld_cli_main(int argc, char **argv);
+
+/* Integer roofline denominator: sustained 32-bit integer ALU operations per
+ * second of the device, from a microbenchmark of independent add/xor
+ * dependency chains (no counterpart in the reference).  *ms gets the
+ * fastest launch time. */
+ld_status ld_measure_int32_peak(int32_t device, double *ops_per_second, double *ms);
+
+/* Last error message of the calling thread ("" if none). */
+const char *ld_last_error(void);
+/* Library version string. */
+const char *ld_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LNORMS_B200_H */

@@ -1,0 +1,323 @@
+"""Python binding of the B200-native exact L_d-norm solver (liblnorms_b200.so).
+
+The stages mirror the reference's pipeline (istvanmarton/L-norms_BruteForce,
+L_CUDA.cu:414-439): read and preprocess a matrix (``Problem``), solve on the
+GPU (``Problem.solve`` / ``solve_reduced`` / ``Plan``), and report the value
+line and the strategy file in the original indexing (``Problem.report``).
+``lnorm`` runs the whole pipeline in one call, like ``./L_CUDA``.
+
+There is no CPU fallback: without the built library or a CUDA device every
+solve raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "lib" / "liblnorms_b200.so"
+CLI_PATH = PKG_DIR / "lib" / "L_CUDA"
+
+LD_OK = 0
+STATUS = {0: "LD_OK", 1: "LD_ERR_ARG", 2: "LD_ERR_INPUT", 3: "LD_ERR_LIMIT", 4: "LD_ERR_CUDA",
+          5: "LD_ERR_NODEV", 6: "LD_ERR_IO", 7: "LD_ERR_TIMEOUT", 8: "LD_ERR_NOMEM"}
+KERNEL_TABLE, KERNEL_WIDE = 1, 2
+
+
+class LdError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Result(C.Structure):
+    _fields_ = [("value", C.c_int64), ("gray_index", C.c_uint64), ("labelings", C.c_uint64),
+                ("kernel_ms", C.c_float), ("kernel_kind", C.c_int32), ("lane_bits", C.c_int32),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32), ("low_rows", C.c_int32), ("threads_per_block", C.c_int32),
+                ("blocks", C.c_int32), ("tile", C.c_int32), ("kernel", C.c_int32),
+                ("lane_bits", C.c_int32), ("shard_index", C.c_int32), ("shard_count", C.c_int32),
+                ("reserved", C.c_int32), ("stream", C.c_void_p)]
+
+
+class ProblemInfo(C.Structure):
+    _fields_ = [("rows_in", C.c_int32), ("cols_in", C.c_int32), ("rows", C.c_int32),
+                ("cols", C.c_int32), ("d_user", C.c_int32), ("d", C.c_int32),
+                ("marginal_user", C.c_int32), ("marginal", C.c_int32), ("transposed", C.c_int32),
+                ("max_rows", C.c_int32), ("labelings", C.c_uint64)]
+
+
+# Every exported symbol of include/lnorms_b200.h: (name, restype, argtypes)
+_P = C.c_void_p
+_I64P = C.POINTER(C.c_int64)
+_I32P = C.POINTER(C.c_int32)
+SIGNATURES = [
+    ("ld_options_init", None, [C.POINTER(Options)]),
+    ("ld_problem_from_text", C.c_int, [C.c_char_p, C.c_size_t, C.c_int32, C.c_char, C.c_int32, C.POINTER(_P)]),
+    ("ld_problem_from_file", C.c_int, [C.c_char_p, C.c_int32, C.c_char, C.c_int32, C.POINTER(_P)]),
+    ("ld_problem_from_matrix", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_char, C.c_int32, C.POINTER(_P)]),
+    ("ld_problem_destroy", None, [_P]),
+    ("ld_problem_get_info", C.c_int, [_P, C.POINTER(ProblemInfo)]),
+    ("ld_problem_reduced", C.c_int, [_P, _I64P, C.c_size_t]),
+    ("ld_problem_log", C.c_char_p, [_P]),
+    ("ld_problem_check_launch", C.c_int, [_P, C.c_int32, C.c_int32]),
+    ("ld_problem_solve", C.c_int, [_P, C.POINTER(Options), C.POINTER(Result)]),
+    ("ld_solve_reduced", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options),
+                                   C.POINTER(Result), _I32P]),
+    ("ld_gray_labels", C.c_int, [C.c_uint64, C.c_int32, C.c_int32, _I32P]),
+    ("ld_problem_report", C.c_int, [_P, C.POINTER(Result), _I32P, C.c_int32, _I32P, C.c_char_p, C.c_size_t]),
+    ("ld_plan_create", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options), C.POINTER(_P)]),
+    ("ld_plan_launch", C.c_int, [_P]),
+    ("ld_plan_result", C.c_int, [_P, C.POINTER(Result), _I32P]),
+    ("ld_plan_range", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("ld_plan_describe", C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    ("ld_plan_stream", C.c_void_p, [_P]),
+    ("ld_plan_result_device", C.c_void_p, [_P]),
+    ("ld_plan_destroy", None, [_P]),
+    ("ld_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+    ("ld_measure_int32_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("ld_last_error", C.c_char_p, []),
+    ("ld_version", C.c_char_p, []),
+]
+
+_lib = None
+
+
+def lib():
+    """The loaded solver library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              f"`make -C {PKG_DIR}` (or __graft_entry__.build())")
+        L = C.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(st: int) -> None:
+    if st != LD_OK:
+        raise LdError(st, lib().ld_last_error().decode(errors="replace"))
+
+
+def options(**kw) -> Options:
+    o = Options()
+    lib().ld_options_init(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _as_i64(a) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+    if a.ndim != 2:
+        raise ValueError("matrix must be 2-D")
+    return a
+
+
+@dataclass
+class Solution:
+    value: int
+    gray_index: int
+    labels: np.ndarray          # labels of reduced rows 0..R-2 (second->strategy)
+    labelings: int
+    kernel_ms: float
+    kernel_kind: int
+    lane_bits: int
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+
+
+def _solution(res: Result, labels: np.ndarray) -> Solution:
+    return Solution(int(res.value), int(res.gray_index), labels, int(res.labelings),
+                    float(res.kernel_ms), int(res.kernel_kind), int(res.lane_bits),
+                    int(res.h2d_bytes), int(res.d2h_bytes))
+
+
+def solve_reduced(a, d: int, marginal: bool = False, opts: Options | None = None) -> Solution:
+    """calc_Lnorm on an already reduced matrix (last row fixed / marginal row)."""
+    a = _as_i64(a)
+    r, c = a.shape
+    labels = np.zeros(max(r - 1, 1), dtype=np.int32)
+    res = Result()
+    _check(lib().ld_solve_reduced(a.ctypes.data_as(_I64P), r, c, d, int(marginal),
+                                  C.byref(opts) if opts is not None else None, C.byref(res),
+                                  labels.ctypes.data_as(_I32P)))
+    return _solution(res, labels[: max(r - 1, 0)])
+
+
+def gray_labels(index: int, rows: int, d: int) -> np.ndarray:
+    out = np.zeros(max(rows - 1, 1), dtype=np.int32)
+    _check(lib().ld_gray_labels(index, rows, d, out.ctypes.data_as(_I32P)))
+    return out[: max(rows - 1, 0)]
+
+
+def int32_peak(device: int = 0):
+    """(sustained int32 ALU ops/s, fastest launch ms) of the device."""
+    ops, ms = C.c_double(), C.c_double()
+    _check(lib().ld_measure_int32_peak(device, C.byref(ops), C.byref(ms)))
+    return float(ops.value), float(ms.value)
+
+
+class Problem:
+    """Read + preprocess (matrix_read and load_parameters of the reference)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_text(cls, text: str | bytes, d: int, stat: str = "n", marginal: bool = False):
+        raw = text.encode() if isinstance(text, str) else text
+        h = C.c_void_p()
+        _check(lib().ld_problem_from_text(raw, len(raw), d, (stat or "n")[0].encode(), int(marginal),
+                                          C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_file(cls, path, d: int, stat: str = "n", marginal: bool = False):
+        h = C.c_void_p()
+        _check(lib().ld_problem_from_file(str(path).encode(), d, (stat or "n")[0].encode(),
+                                          int(marginal), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_matrix(cls, a, d: int, stat: str = "n", marginal: bool = False):
+        a = _as_i64(a)
+        h = C.c_void_p()
+        _check(lib().ld_problem_from_matrix(a.ctypes.data_as(_I64P), a.shape[0], a.shape[1], d,
+                                            (stat or "n")[0].encode(), int(marginal), C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.ld_problem_destroy(h)
+            self._h = None
+
+    @property
+    def info(self) -> dict:
+        inf = ProblemInfo()
+        _check(lib().ld_problem_get_info(self._h, C.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in ProblemInfo._fields_}
+
+    @property
+    def reduced(self) -> np.ndarray:
+        inf = self.info
+        out = np.zeros(max(inf["rows"] * inf["cols"], 1), dtype=np.int64)
+        _check(lib().ld_problem_reduced(self._h, out.ctypes.data_as(_I64P), out.size))
+        return out[: inf["rows"] * inf["cols"]].reshape(inf["rows"], inf["cols"])
+
+    @property
+    def log(self) -> str:
+        return lib().ld_problem_log(self._h).decode()
+
+    def check_launch(self, blocks: int = 512, threads: int = 32) -> None:
+        _check(lib().ld_problem_check_launch(self._h, blocks, threads))
+
+    def solve(self, opts: Options | None = None) -> Result:
+        res = Result()
+        _check(lib().ld_problem_solve(self._h, C.byref(opts) if opts is not None else None,
+                                      C.byref(res)))
+        return res
+
+    def report(self, res: Result):
+        """(value line appended to the log, strategy file name, strategy file text)."""
+        n = max(self.info["rows_in"], self.info["cols_in"])
+        strat = np.zeros(max(n, 1), dtype=np.int32)
+        cnt = C.c_int32()
+        name = C.create_string_buffer(64)
+        _check(lib().ld_problem_report(self._h, C.byref(res), strat.ctypes.data_as(_I32P), strat.size,
+                                       C.byref(cnt), name, len(name)))
+        text = "".join(f"{int(v)}\n" for v in strat[: cnt.value])
+        return name.value.decode(), text
+
+
+def lnorm(source, d: int, stat: str = "n", marginal: bool = False, blocks: int = 512,
+          threads: int = 32, opts: Options | None = None):
+    """Whole pipeline (like ./L_CUDA): returns (value, stdout_text, strategy_name, strategy_text)."""
+    if isinstance(source, (str, os.PathLike)) and Path(source).exists():
+        p = Problem.from_file(source, d, stat, marginal)
+    elif isinstance(source, (str, bytes)):
+        p = Problem.from_text(source, d, stat, marginal)
+    else:
+        p = Problem.from_matrix(source, d, stat, marginal)
+    p.check_launch(blocks, threads)
+    if p.info["rows"] == 0:
+        res = Result()
+        zero = True
+    else:
+        res = p.solve(opts)
+        zero = False
+    name, text = p.report(res)
+    out = p.log
+    if zero:  # main() prints this line itself, before the value (L_CUDA.cu:432)
+        lines = out.splitlines(keepends=True)
+        out = "".join(lines[:-1]) + "This is a zero matrix.\n" + lines[-1]
+    return int(res.value), out, name, text
+
+
+class Plan:
+    """A device-resident reduced matrix for repeated solves."""
+
+    def __init__(self, a, d: int, marginal: bool = False, opts: Options | None = None):
+        a = _as_i64(a)
+        self.rows, self.cols = a.shape
+        self.d = d
+        h = C.c_void_p()
+        _check(lib().ld_plan_create(a.ctypes.data_as(_I64P), a.shape[0], a.shape[1], d, int(marginal),
+                                    C.byref(opts) if opts is not None else None, C.byref(h)))
+        self._h = h
+
+    def launch(self) -> None:
+        _check(lib().ld_plan_launch(self._h))
+
+    def result(self) -> Solution:
+        res = Result()
+        labels = np.zeros(max(self.rows - 1, 1), dtype=np.int32)
+        _check(lib().ld_plan_result(self._h, C.byref(res), labels.ctypes.data_as(_I32P)))
+        return _solution(res, labels[: max(self.rows - 1, 0)])
+
+    def solve(self) -> Solution:
+        self.launch()
+        return self.result()
+
+    @property
+    def range(self):
+        lo, hi = C.c_uint64(), C.c_uint64()
+        _check(lib().ld_plan_range(self._h, C.byref(lo), C.byref(hi)))
+        return int(lo.value), int(hi.value)
+
+    @property
+    def stream(self) -> int:
+        return int(lib().ld_plan_stream(self._h) or 0)
+
+    @property
+    def result_device_ptr(self) -> int:
+        """Device address of the 16-byte {value, index} result of the last launch."""
+        return int(lib().ld_plan_result_device(self._h) or 0)
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(256)
+        _check(lib().ld_plan_describe(self._h, buf, len(buf)))
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ld_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ld_plan_destroy(self._h)
+            self._h = None

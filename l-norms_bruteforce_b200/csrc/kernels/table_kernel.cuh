@@ -1,0 +1,298 @@
+// Table enumeration kernel for L_1, LM (d = 1), L_2 and L_3.
+//
+// The Gray index of a labeling is split as N = h * B + j, B = d^k: the k
+// lowest free rows ("low rows", digits of j) and the rest ("high rows",
+// digits of h).  For the d-ary reflected Gray code used by the reference
+// (binary for d <= 2, L_CUDA.cu:61-63; pattern 0..d-1,d-1..0 for d >= 3,
+// L_CUDA.cu:204-206), the high rows' labels are the Gray word of h and the
+// low rows' labels are the Gray word of j, read backwards (B-1-j) when h is
+// odd.  So every block of B consecutive indices visits all B low labelings.
+//
+// Each block tabulates, once, the low rows' contribution to the message
+// column sums for all B low labelings (Gray order, shared memory).  Each
+// thread keeps the high rows' column sums H in registers, walks h in Gray
+// order (one row changes per step: one packed add or subtract of a row
+// staged in shared memory), and for every h evaluates all B labelings as
+//     sum over message vectors and columns of |H + L_j|
+// with one packed absolute-difference-accumulate per column word against
+// the tabulated entry (a warp-uniform broadcast read).  With PK columns per
+// 32-bit word (int8x4 / int16x2 / int32 lanes, chosen by the host from an
+// exact bound) one instruction covers PK columns.
+//
+// Message vectors per labeling (NV = D):
+//   D = 1 (L_1 / LM): s = A_fixed + sum s_i A_i;          table: -L
+//   D = 2 (L_2):      s1 = rows labelled 1, s0 = T - s1;   table: -L1, T-L1
+//   D = 3 (L_3):      s1, s2, s0 = T - s1 - s2;            table: -L1, -L2, T-L1-L2
+//     with registers H1, H2 and H1+H2 for D = 3.
+// LM enters as L_1 with column 0 shifted by K = sum_i |A_i0| (host side),
+// which makes that column's term equal to its signed sum plus K.
+#pragma once
+#include "common.cuh"
+
+namespace ld {
+
+struct TableArgs {
+  const uint32_t* A;        // R x W packed rows; row R-1 is the fixed row
+  const uint32_t* tot;      // W words: column totals over all rows (D >= 2)
+  const uint32_t* hinit;    // W words: H before any high row (D = 1: fixed row)
+  int R;                    // reduced rows
+  int k;                    // low rows (tabulated)
+  int B;                    // d^k
+  int fw;                   // Gray digits walked per seed (walk length d^fw)
+  unsigned long long walk_len;
+  unsigned long long walk_begin, walk_end;  // walks of this launch
+  long long value_offset;   // subtracted from every value (LM shift K)
+  Reduce red;
+};
+
+constexpr int kTableThreads = 128;
+
+__host__ __device__ constexpr int table_words(int D, int W) { return D * W; }
+
+// Shared memory: packed rows, totals, initial H, then the table (16-byte
+// aligned).
+__host__ __device__ inline int table_smem_words(int D, int W, int R, int B) {
+  int head = R * W + 2 * W;
+  head = (head + 3) & ~3;
+  return head + B * D * W;
+}
+
+template <int D, int W, int PK>
+__device__ __forceinline__ void add_row(uint32_t* H, const uint32_t* row, int vec) {
+  using L = Lanes<PK>;
+#pragma unroll
+  for (int w = 0; w < W; ++w) H[vec * W + w] = L::add(H[vec * W + w], row[w]);
+}
+
+template <int D, int W, int PK>
+__device__ __forceinline__ void sub_row(uint32_t* H, const uint32_t* row, int vec) {
+  using L = Lanes<PK>;
+#pragma unroll
+  for (int w = 0; w < W; ++w) H[vec * W + w] = L::sub(H[vec * W + w], row[w]);
+}
+
+// Move high row r from label a to label b.
+template <int D, int W, int PK>
+__device__ __forceinline__ void move_row(uint32_t* H, const uint32_t* row, int a, int b) {
+  if (D == 1) {  // sign a -> b: add or subtract 2 * row (as two steps, each in range)
+    if (b) { add_row<D, W, PK>(H, row, 0); add_row<D, W, PK>(H, row, 0); }
+    else   { sub_row<D, W, PK>(H, row, 0); sub_row<D, W, PK>(H, row, 0); }
+  } else if (D == 2) {
+    if (b) add_row<D, W, PK>(H, row, 0); else sub_row<D, W, PK>(H, row, 0);
+  } else {
+    if (a == 1) sub_row<D, W, PK>(H, row, 0);
+    if (a == 2) sub_row<D, W, PK>(H, row, 1);
+    if (b == 1) add_row<D, W, PK>(H, row, 0);
+    if (b == 2) add_row<D, W, PK>(H, row, 1);
+    if (a == 0 && b != 0) add_row<D, W, PK>(H, row, 2);
+    if (a != 0 && b == 0) sub_row<D, W, PK>(H, row, 2);
+  }
+}
+
+// H for high index h: initial vector plus every high row at its label.
+template <int D, int W, int PK>
+__device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const uint32_t* sH0,
+                                          int k, int nh, unsigned long long h) {
+  constexpr int NV = D;
+#pragma unroll
+  for (int w = 0; w < W; ++w) H[w] = sH0[w];
+#pragma unroll
+  for (int v = 1; v < NV; ++v)
+#pragma unroll
+    for (int w = 0; w < W; ++w) H[v * W + w] = 0u;
+  if (D <= 2) {
+    const unsigned long long g = h ^ (h >> 1);
+    for (int t = 0; t < nh; ++t) {
+      const int lab = (int)((g >> t) & 1ull);
+      const uint32_t* row = sA + (k + t) * W;
+      if (D == 1) { if (lab) add_row<D, W, PK>(H, row, 0); else sub_row<D, W, PK>(H, row, 0); }
+      else if (lab) add_row<D, W, PK>(H, row, 0);
+    }
+  } else {
+    unsigned long long q = h;
+    for (int t = 0; t < nh; ++t) {
+      const int r = (int)(q % 6ull);
+      const int lab = r < 3 ? r : 5 - r;
+      q /= 3ull;
+      const uint32_t* row = sA + (k + t) * W;
+      if (lab == 1) { add_row<D, W, PK>(H, row, 0); add_row<D, W, PK>(H, row, 2); }
+      else if (lab == 2) { add_row<D, W, PK>(H, row, 1); add_row<D, W, PK>(H, row, 2); }
+    }
+  }
+}
+
+// Value of table entry e against H.
+template <int D, int W, int PK>
+__device__ __forceinline__ int entry_value(const uint32_t* H, const uint32_t* e) {
+  using L = Lanes<PK>;
+  constexpr int NW = D * W;
+  const uint4* t = reinterpret_cast<const uint4*>(e);
+  uint32_t a0 = 0u, a1 = 0u;
+#pragma unroll
+  for (int q = 0; q < NW / 4; ++q) {
+    const uint4 x = t[q];
+    a0 = L::sad(H[4 * q + 0], x.x, a0);
+    a1 = L::sad(H[4 * q + 1], x.y, a1);
+    a0 = L::sad(H[4 * q + 2], x.z, a0);
+    a1 = L::sad(H[4 * q + 3], x.w, a1);
+  }
+  return (int)(a0 + a1);
+}
+
+// max over all B table entries
+template <int D, int W, int PK>
+__device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, int B) {
+  using L = Lanes<PK>;
+  constexpr int NW = D * W;
+  int m = INT_MIN;
+  int j = 0;
+  for (; j + 2 <= B; j += 2) {
+    const uint4* t0 = reinterpret_cast<const uint4*>(sT + j * NW);
+    const uint4* t1 = reinterpret_cast<const uint4*>(sT + (j + 1) * NW);
+    uint32_t a0 = 0u, a1 = 0u, b0 = 0u, b1 = 0u;
+#pragma unroll
+    for (int q = 0; q < NW / 4; ++q) {
+      const uint4 x = t0[q];
+      const uint4 y = t1[q];
+      a0 = L::sad(H[4 * q + 0], x.x, a0);
+      b0 = L::sad(H[4 * q + 0], y.x, b0);
+      a1 = L::sad(H[4 * q + 1], x.y, a1);
+      b1 = L::sad(H[4 * q + 1], y.y, b1);
+      a0 = L::sad(H[4 * q + 2], x.z, a0);
+      b0 = L::sad(H[4 * q + 2], y.z, b0);
+      a1 = L::sad(H[4 * q + 3], x.w, a1);
+      b1 = L::sad(H[4 * q + 3], y.w, b1);
+    }
+    m = max(m, max((int)(a0 + a1), (int)(b0 + b1)));
+  }
+  if (j < B) m = max(m, entry_value<D, W, PK>(H, sT + j * NW));
+  return m;
+}
+
+template <int D, int W, int PK>
+__global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs args) {
+  constexpr int NW = D * W;
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int R = args.R, k = args.k, B = args.B;
+  const int nh = R - 1 - k;  // high rows
+  uint32_t* sA = smem;
+  uint32_t* sTot = sA + R * W;
+  uint32_t* sH0 = sTot + W;
+  uint32_t* sT = smem + (((R * W + 2 * W) + 3) & ~3);
+
+  for (int t = threadIdx.x; t < R * W; t += blockDim.x) sA[t] = args.A[t];
+  for (int t = threadIdx.x; t < W; t += blockDim.x) { sTot[t] = args.tot[t]; sH0[t] = args.hinit[t]; }
+  __syncthreads();
+
+  // Tabulate the low rows' partial sums for every low labeling j (Gray order).
+  for (int j = threadIdx.x; j < B; j += blockDim.x) {
+    uint32_t L1[W], L2[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) { L1[w] = 0u; L2[w] = 0u; }
+    if (D <= 2) {
+      const unsigned g = (unsigned)j ^ ((unsigned)j >> 1);
+      for (int i = 0; i < k; ++i) {
+        const int lab = (g >> i) & 1u;
+        const uint32_t* row = sA + i * W;
+        if (D == 1) {
+          // entry = -(sum s_i A_i): subtract rows labelled +1, add rows labelled -1
+#pragma unroll
+          for (int w = 0; w < W; ++w) L1[w] = lab ? Lanes<PK>::sub(L1[w], row[w]) : Lanes<PK>::add(L1[w], row[w]);
+        } else if (lab) {
+#pragma unroll
+          for (int w = 0; w < W; ++w) L1[w] = Lanes<PK>::add(L1[w], row[w]);
+        }
+      }
+    } else {
+      unsigned q = (unsigned)j;
+      for (int i = 0; i < k; ++i) {
+        const unsigned r = q % 6u;
+        const int lab = r < 3u ? (int)r : 5 - (int)r;
+        q /= 3u;
+        const uint32_t* row = sA + i * W;
+        if (lab == 1) {
+#pragma unroll
+          for (int w = 0; w < W; ++w) L1[w] = Lanes<PK>::add(L1[w], row[w]);
+        } else if (lab == 2) {
+#pragma unroll
+          for (int w = 0; w < W; ++w) L2[w] = Lanes<PK>::add(L2[w], row[w]);
+        }
+      }
+    }
+    uint32_t* e = sT + j * NW;
+    if (D == 1) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) e[w] = L1[w];
+    } else if (D == 2) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        e[w] = Lanes<PK>::sub(0u, L1[w]);
+        e[W + w] = Lanes<PK>::sub(sTot[w], L1[w]);
+      }
+    } else {
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        e[w] = Lanes<PK>::sub(0u, L1[w]);
+        e[W + w] = Lanes<PK>::sub(0u, L2[w]);
+        e[2 * W + w] = Lanes<PK>::sub(Lanes<PK>::sub(sTot[w], L1[w]), L2[w]);
+      }
+    }
+  }
+  __syncthreads();
+
+  // Walk high indices: walks w, w + T, ... each covering walk_len
+  // consecutive (aligned) high indices, so the changed row is warp-uniform.
+  const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long WL = args.walk_len;
+  uint32_t H[NW];
+  int best = INT_MIN;
+  unsigned long long best_h = 0ull;
+  for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += T) {
+    const unsigned long long h0 = wk * WL;
+    seed_high<D, W, PK>(H, sA, sH0, k, nh, h0);
+    for (unsigned long long u = 0; u < WL; ++u) {
+      if (u) {
+        const unsigned long long h = h0 + u;
+        int i, a, b;
+        if (D <= 2) {
+          i = __ffsll((long long)u) - 1;            // == ctz(h): h0 is a multiple of 2^fw
+          b = (int)(((h >> (i + 1)) & 1ull) ^ 1ull);
+          a = b ^ 1;
+        } else {
+          unsigned long long q = u;
+          i = 0;
+          while (q % 3ull == 0ull) { q /= 3ull; ++i; }
+          const int c = (int)(q % 3ull);
+          // parity of h / 3^(i+1) = parity of wk (times an odd power) + u / 3^(i+1)
+          const int par = (int)((wk ^ (q / 3ull)) & 1ull);
+          b = par ? 2 - c : c;
+          a = par ? 3 - c : c - 1;
+        }
+        move_row<D, W, PK>(H, sA + (k + i) * W, a, b);
+      }
+      const int m = scan_max<D, W, PK>(H, sT, B);
+      if (m > best) { best = m; best_h = h0 + u; }
+    }
+  }
+
+  // The first index attaining the thread's best: rescan its block in the
+  // Gray order of the low part (reversed for odd h).
+  long long bv = LLONG_MIN;
+  unsigned long long bn = ULLONG_MAX;
+  if (best != INT_MIN) {
+    seed_high<D, W, PK>(H, sA, sH0, k, nh, best_h);
+    const bool rev = (best_h & 1ull) != 0ull;
+    for (int jj = 0; jj < B; ++jj) {
+      const int je = rev ? B - 1 - jj : jj;
+      if (entry_value<D, W, PK>(H, sT + je * NW) == best) {
+        bn = best_h * (unsigned long long)B + (unsigned long long)jj;
+        break;
+      }
+    }
+    bv = (long long)best - args.value_offset;
+  }
+  grid_reduce(bv, bn, args.red);
+}
+
+}  // namespace ld

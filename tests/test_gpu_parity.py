@@ -1,0 +1,176 @@
+"""Parity of the CUDA path with the oracle and the reference's own outputs.
+
+Everything goes through the C-ABI (ctypes) or the drop-in executable.  The
+bar is bit-exact: the same value and the same (smallest) Gray index, hence
+the same strategy file.
+"""
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+from helpers import GOLDEN, split_tail, without_launch_line
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=[c["name"] for c in GOLDEN])
+def test_pipeline_matches_reference(ld, case):
+    d, stat, marg = split_tail(case["tail"])
+    value, out, name, strat = ld.lnorm(case["text"], d, stat, marg, 512, 32)
+    assert without_launch_line(out) == without_launch_line(case["stdout"])
+    assert name == case["strategy_name"]
+    assert strat == case["strategy"]
+
+
+CLI_CASES = [c for c in GOLDEN if c["name"].startswith(("config", "chsh", "reset", "marg_", "zero",
+                                                       "single", "sci", "separators", "mid_", "wide_"))]
+
+
+@pytest.mark.parametrize("case", CLI_CASES, ids=[c["name"] for c in CLI_CASES])
+def test_cli_matches_reference(ld, case, tmp_path):
+    (tmp_path / "m.txt").write_text(case["text"])
+    p = subprocess.run([str(ld.CLI_PATH), "512", "32", "m.txt", *case["tail"]], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    assert without_launch_line(p.stdout) == without_launch_line(case["stdout"])
+    files = list(tmp_path.glob("strategy_*.txt"))
+    assert [f.name for f in files] == [case["strategy_name"]]
+    assert files[0].read_text() == case["strategy"]
+
+
+def random_case(seed):
+    rng = np.random.default_rng(1000 + seed)
+    d = int(rng.choice([1, 1, 1, 2, 2, 3, 3, 4, 5, 6, 8, 10]))
+    maxr = {1: 22, 2: 21, 3: 13, 4: 10, 5: 9, 6: 8, 8: 7, 10: 6}[d]
+    r = int(rng.integers(1, maxr + 1))
+    c = int(rng.choice([1, 2, 3, 5, 8, 13, 24, 31, 40, 64, 65, 100]))
+    amp = int(rng.choice([1, 3, 20, 300, 40000]))
+    a = rng.integers(-amp, amp + 1, size=(r, c)).astype(np.int64)
+    marg = d == 1 and rng.random() < 0.3
+    return a, d, marg
+
+
+@pytest.mark.parametrize("seed", range(120))
+def test_random_against_oracle(ld, seed):
+    a, d, marg = random_case(seed)
+    sol = ld.solve_reduced(a, d, marg)
+    v, n = O.enumerate_max(a, d, marg)
+    assert (sol.value, sol.gray_index) == (v, n)
+    assert np.array_equal(sol.labels, O.labels(n, a.shape[0], d))
+    assert sol.labelings == O.total(a.shape[0], d)
+
+
+FORCED = [dict(kernel=1, lane_bits=8), dict(kernel=1, lane_bits=16), dict(kernel=1, lane_bits=32),
+          dict(kernel=2, lane_bits=32), dict(kernel=2, lane_bits=64),
+          dict(kernel=1, low_rows=0), dict(kernel=1, low_rows=1), dict(kernel=1, low_rows=3, tile=2),
+          dict(kernel=1, blocks=1), dict(kernel=1, blocks=3, tile=1), dict(kernel=2, blocks=1)]
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("marg", [False, True])
+@pytest.mark.parametrize("forced", FORCED, ids=[str(f) for f in FORCED])
+def test_every_kernel_path(ld, d, marg, forced):
+    if marg and d != 1:
+        pytest.skip("marginals are d == 1 only")
+    rng = np.random.default_rng(d * 7 + marg)
+    r = {1: 17, 2: 16, 3: 11}[d]
+    a = rng.integers(-3, 4, size=(r, 9)).astype(np.int64)
+    if forced.get("lane_bits") == 8 and marg:
+        a[:, 0] = rng.integers(-1, 2, size=r)   # keep 2*sum|A_i0| within int8
+    sol = ld.solve_reduced(a, d, marg, ld.options(**forced))
+    v, n = O.enumerate_max(a, d, marg)
+    assert (sol.value, sol.gray_index) == (v, n)
+    if "lane_bits" in forced:
+        assert sol.lane_bits == forced["lane_bits"]
+    assert sol.kernel_kind == forced["kernel"]
+
+
+@pytest.mark.parametrize("d", [1, 2, 3, 4])
+def test_ties_resolve_to_smallest_index(ld, d):
+    """Many labelings share the maximum; the reported index must be the
+    first in Gray order (strict '>' per worker, strict '<' across workers)."""
+    a = np.ones((9 if d < 4 else 7, 4), dtype=np.int64)
+    a[::2] *= -1
+    for opts in (ld.options(), ld.options(blocks=1), ld.options(kernel=2)):
+        sol = ld.solve_reduced(a, d, False, opts)
+        assert (sol.value, sol.gray_index) == O.enumerate_max(a, d, False)
+
+
+def test_int64_entries(ld):
+    rng = np.random.default_rng(5)
+    for d in (1, 2, 3, 5):
+        a = rng.integers(-2**40, 2**40, size=(8, 6)).astype(np.int64)
+        sol = ld.solve_reduced(a, d)
+        assert sol.lane_bits == 64
+        assert (sol.value, sol.gray_index) == O.enumerate_max(a, d, False)
+    # int32 entries whose column sums overflow int32
+    a = rng.integers(2**30, 2**31 - 1, size=(10, 5)).astype(np.int64)
+    sol = ld.solve_reduced(a, 1)
+    assert sol.value > 2**31 and sol.lane_bits == 64
+    assert (sol.value, sol.gray_index) == O.enumerate_max(a, 1, False)
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("count", [2, 3, 5])
+def test_shards_tile_the_index_space(ld, kernel, count):
+    rng = np.random.default_rng(count)
+    a = rng.integers(-9, 10, size=(19, 23)).astype(np.int64)
+    full = O.enumerate_max(a, 1, False)
+    parts, ranges = [], []
+    for s in range(count):
+        plan = ld.Plan(a, 1, False, ld.options(kernel=kernel, shard_index=s, shard_count=count))
+        lo, hi = plan.range
+        sol = plan.solve()
+        assert (sol.value, sol.gray_index) == O.enumerate_max(a, 1, False, lo, hi)
+        parts.append((sol.value, -sol.gray_index))
+        ranges.append((lo, hi))
+        plan.close()
+    assert ranges[0][0] == 0 and ranges[-1][1] == O.total(19, 1)
+    assert all(ranges[i][1] == ranges[i + 1][0] for i in range(count - 1))
+    best = max(parts)
+    assert (best[0], -best[1]) == full
+
+
+def test_plan_relaunch_is_stable(ld):
+    rng = np.random.default_rng(9)
+    a = rng.integers(-20, 21, size=(26, 30)).astype(np.int64)
+    plan = ld.Plan(a, 1)
+    first = plan.solve()
+    for _ in range(3):
+        again = plan.solve()
+        assert (again.value, again.gray_index) == (first.value, first.gray_index)
+        assert again.kernel_ms > 0
+    plan.close()
+    assert (first.value, first.gray_index) == O.enumerate_max(a, 1, False)
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 7), (2, 1), (2, 2), (3, 1), (5, 130), (12, 2100), (4, 4096)])
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_edge_shapes(ld, shape, d):
+    rng = np.random.default_rng(shape[0] * 1000 + shape[1] + d)
+    a = rng.integers(-50, 51, size=shape).astype(np.int64)
+    sol = ld.solve_reduced(a, d)
+    assert (sol.value, sol.gray_index) == O.enumerate_max(a, d, False)
+
+
+def test_full_size_witness_and_invariances(ld, workloads):
+    """At sizes the oracle cannot enumerate: the returned index is a witness
+    of the value, and the value is invariant under column permutation and
+    column negation, and under negating a free row (d = 1)."""
+    a = workloads.lowrank(36, 44, np.random.default_rng(77))
+    base = ld.solve_reduced(a, 1)
+    assert O.value(a, 1, False, O.labels(base.gray_index, 36, 1)) == base.value
+    rng = np.random.default_rng(1)
+    perm = rng.permutation(44)
+    sign = rng.choice([-1, 1], size=44)
+    b = a[:, perm] * sign[None, :]
+    assert ld.solve_reduced(b, 1).value == base.value
+    c = a.copy()
+    c[3] *= -1
+    assert ld.solve_reduced(c, 1).value == base.value
+    # sharded over 4 = whole
+    parts = [ld.solve_reduced(a, 1, False, ld.options(shard_index=s, shard_count=4)) for s in range(4)]
+    best = max((p.value, -p.gray_index) for p in parts)
+    assert (best[0], -best[1]) == (base.value, base.gray_index)

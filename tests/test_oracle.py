@@ -1,33 +1,12 @@
 """The oracle (CPU restatement) against the reference's own outputs and
 against an independent pure-Python brute force on tiny cases."""
 import itertools
-import json
-from pathlib import Path
 
 import numpy as np
 import pytest
 
 import oracle_ffi as O
-
-GOLDEN = json.loads((Path(__file__).parent / "golden" / "cases.json").read_text())
-
-
-def split_tail(tail):
-    """argv tail -> (d, stat, marginal) exactly as arguments_CUDA reads it
-    (L_CUDA.cu:392-409)."""
-    d = int(tail[0])
-    stat = tail[1][0] if len(tail) > 1 else "n"
-    marg = False
-    if d == 1 and len(tail) == 2:
-        marg = tail[1][0] in "mM"
-    elif d == 1 and len(tail) >= 3:
-        marg = tail[2][0] in "mM"
-    return d, stat, marg
-
-
-def lines_without_launch(s):
-    return [ln for ln in s.splitlines()
-            if not ln.startswith("number of threads:") and not ln.startswith("num_ofBlock:")]
+from helpers import GOLDEN, split_tail, without_launch_line as lines_without_launch
 
 
 @pytest.mark.parametrize("case", GOLDEN, ids=[c["name"] for c in GOLDEN])
