@@ -243,10 +243,21 @@ class Problem:
         return name.value.decode(), text
 
 
+def _is_path(source) -> bool:
+    if isinstance(source, os.PathLike):
+        return True
+    if isinstance(source, str) and "\n" not in source:
+        try:
+            return Path(source).is_file()
+        except OSError:
+            return False
+    return False
+
+
 def lnorm(source, d: int, stat: str = "n", marginal: bool = False, blocks: int = 512,
           threads: int = 32, opts: Options | None = None):
     """Whole pipeline (like ./L_CUDA): returns (value, stdout_text, strategy_name, strategy_text)."""
-    if isinstance(source, (str, os.PathLike)) and Path(source).exists():
+    if _is_path(source):
         p = Problem.from_file(source, d, stat, marginal)
     elif isinstance(source, (str, bytes)):
         p = Problem.from_text(source, d, stat, marginal)

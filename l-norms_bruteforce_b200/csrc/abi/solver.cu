@@ -78,14 +78,15 @@ ld_status choose_kernel(int R, int C, int d, int marginal, const Bounds& b, cons
   const long long vmax = b.total + (marginal ? b.K : 0LL);
   const bool fits32 = vmax <= (long long)INT32_MAX && maxabs <= (long long)INT32_MAX;
   if (o.kernel != LD_KERNEL_WIDE && d <= 3 && o.lane_bits != 64) {
-    const int cand[3] = {4, 2, 1};
+    const int cand[2] = {4, 1};
     for (int pk : cand) {
       const int bits = 32 / pk;
       if (o.lane_bits && o.lane_bits != bits) continue;
-      const long long lim = pk == 4 ? 127 : pk == 2 ? 32767 : (long long)INT32_MAX;
+      const long long lim = pk == 4 ? 127 : (long long)INT32_MAX;
       if (maxabs > lim || !fits32) continue;
       const int W = round4((C + pk - 1) / pk);
-      if (W > 32 || d * W > 96) continue;
+      const int wmax = pk == 4 ? 32 : (d == 1 ? 64 : d == 2 ? 48 : 32);
+      if (W > wmax) continue;
       ch->kind = LD_KERNEL_TABLE; ch->D = d; ch->W = W; ch->PK = pk; ch->lane_bits = bits;
       return LD_OK;
     }
@@ -95,8 +96,10 @@ ld_status choose_kernel(int R, int C, int d, int marginal, const Bounds& b, cons
   ch->kind = LD_KERNEL_WIDE;
   ch->i64 = (!fits32 || o.lane_bits == 64) ? 1 : 0;
   ch->lane_bits = ch->i64 ? 64 : 32;
-  if (o.lane_bits == 16 || o.lane_bits == 8)
-    return ld_fail(LD_ERR_ARG, "%d-bit lanes need the table kernel", o.lane_bits);
+  if (o.lane_bits == 8)
+    return ld_fail(LD_ERR_ARG, "8-bit lanes need the table kernel");
+  if (o.lane_bits && o.lane_bits != 32 && o.lane_bits != 64)
+    return ld_fail(LD_ERR_ARG, "lane width %d is not 8, 32 or 64", o.lane_bits);
   int pc = 1;
   while (pc * 32 < C) pc *= 2;
   ch->PC = pc;

@@ -1,4 +1,5 @@
-// table_kernel instances for D = 1.
+// table_kernel instances for D = 1: int32 lanes (PK = 1) for W = 4..64 words,
+// int8x4 lanes (PK = 4) for W = 4..32 words.
 #include <utility>
 
 #include "registry.h"
@@ -14,10 +15,8 @@ static const void* pick_d1(int W, std::integer_sequence<int, Ws...>) {
 }
 
 const void* table_kernel_ptr_d1(int W, int PK) {
-  using Seq = std::make_integer_sequence<int, 8>;
-  if (PK == 1) return pick_d1<1>(W, Seq{});
-  if (PK == 2) return pick_d1<2>(W, Seq{});
-  if (PK == 4) return pick_d1<4>(W, Seq{});
+  if (PK == 1) return pick_d1<1>(W, std::make_integer_sequence<int, 16>{});
+  if (PK == 4) return pick_d1<4>(W, std::make_integer_sequence<int, 8>{});
   return nullptr;
 }
 

@@ -62,7 +62,7 @@ def test_random_against_oracle(ld, seed):
     assert sol.labelings == O.total(a.shape[0], d)
 
 
-FORCED = [dict(kernel=1, lane_bits=8), dict(kernel=1, lane_bits=16), dict(kernel=1, lane_bits=32),
+FORCED = [dict(kernel=1, lane_bits=8), dict(kernel=1, lane_bits=32),
           dict(kernel=2, lane_bits=32), dict(kernel=2, lane_bits=64),
           dict(kernel=1, low_rows=0), dict(kernel=1, low_rows=1), dict(kernel=1, low_rows=3, tile=2),
           dict(kernel=1, blocks=1), dict(kernel=1, blocks=3, tile=1), dict(kernel=2, blocks=1)]
