@@ -22,8 +22,10 @@
 // Message vectors per labeling (NV = D):
 //   D = 1 (L_1 / LM): s = A_fixed + sum s_i A_i;          table: -L
 //   D = 2 (L_2):      s1 = rows labelled 1, s0 = T - s1;   table: -L1, T-L1
+//     both table vectors are compared against the same register vector H
+//     (|H + L1| + |H - (T - L1)|);
 //   D = 3 (L_3):      s1, s2, s0 = T - s1 - s2;            table: -L1, -L2, T-L1-L2
-//     with registers H1, H2 and H1+H2 for D = 3.
+//     with registers H1, H2 and H1+H2.
 // LM enters as L_1 with column 0 shifted by K = sum_i |A_i0| (host side),
 // which makes that column's term equal to its signed sum plus K.
 #pragma once
@@ -48,6 +50,11 @@ struct TableArgs {
 constexpr int kTableThreads = 128;
 
 __host__ __device__ constexpr int table_words(int D, int W) { return D * W; }
+// register words of H: one vector for D <= 2, three for D = 3
+__host__ __device__ constexpr int reg_words(int D, int W) { return D == 3 ? 3 * W : W; }
+// register word that table word q is compared with
+template <int D, int W>
+__device__ __forceinline__ constexpr int hword(int q) { return D == 2 ? q % W : q; }
 
 // Shared memory: packed rows, totals, initial H, then the table (16-byte
 // aligned).
@@ -93,7 +100,7 @@ __device__ __forceinline__ void move_row(uint32_t* H, const uint32_t* row, int a
 template <int D, int W, int PK>
 __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const uint32_t* sH0,
                                           int k, int nh, unsigned long long h) {
-  constexpr int NV = D;
+  constexpr int NV = D == 3 ? 3 : 1;
 #pragma unroll
   for (int w = 0; w < W; ++w) H[w] = sH0[w];
 #pragma unroll
@@ -131,10 +138,10 @@ __device__ __forceinline__ int entry_value(const uint32_t* H, const uint32_t* e)
 #pragma unroll
   for (int q = 0; q < NW / 4; ++q) {
     const uint4 x = t[q];
-    a0 = L::sad(H[4 * q + 0], x.x, a0);
-    a1 = L::sad(H[4 * q + 1], x.y, a1);
-    a0 = L::sad(H[4 * q + 2], x.z, a0);
-    a1 = L::sad(H[4 * q + 3], x.w, a1);
+    a0 = L::sad(H[hword<D, W>(4 * q + 0)], x.x, a0);
+    a1 = L::sad(H[hword<D, W>(4 * q + 1)], x.y, a1);
+    a0 = L::sad(H[hword<D, W>(4 * q + 2)], x.z, a0);
+    a1 = L::sad(H[hword<D, W>(4 * q + 3)], x.w, a1);
   }
   return (int)(a0 + a1);
 }
@@ -154,14 +161,16 @@ __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, i
     for (int q = 0; q < NW / 4; ++q) {
       const uint4 x = t0[q];
       const uint4 y = t1[q];
-      a0 = L::sad(H[4 * q + 0], x.x, a0);
-      b0 = L::sad(H[4 * q + 0], y.x, b0);
-      a1 = L::sad(H[4 * q + 1], x.y, a1);
-      b1 = L::sad(H[4 * q + 1], y.y, b1);
-      a0 = L::sad(H[4 * q + 2], x.z, a0);
-      b0 = L::sad(H[4 * q + 2], y.z, b0);
-      a1 = L::sad(H[4 * q + 3], x.w, a1);
-      b1 = L::sad(H[4 * q + 3], y.w, b1);
+      const uint32_t h0 = H[hword<D, W>(4 * q + 0)], h1 = H[hword<D, W>(4 * q + 1)];
+      const uint32_t h2 = H[hword<D, W>(4 * q + 2)], h3 = H[hword<D, W>(4 * q + 3)];
+      a0 = L::sad(h0, x.x, a0);
+      b0 = L::sad(h0, y.x, b0);
+      a1 = L::sad(h1, x.y, a1);
+      b1 = L::sad(h1, y.y, b1);
+      a0 = L::sad(h2, x.z, a0);
+      b0 = L::sad(h2, y.z, b0);
+      a1 = L::sad(h3, x.w, a1);
+      b1 = L::sad(h3, y.w, b1);
     }
     m = max(m, max((int)(a0 + a1), (int)(b0 + b1)));
   }
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
   const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long WL = args.walk_len;
-  uint32_t H[NW];
+  uint32_t H[reg_words(D, W)];
   int best = INT_MIN;
   unsigned long long best_h = 0ull;
   for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += T) {

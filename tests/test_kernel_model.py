@@ -1,0 +1,70 @@
+"""A numpy model of the table kernel's arithmetic, checked against the
+oracle on the CPU.  It pins the decomposition the CUDA kernel relies on:
+N = h * B + j with the high rows' labels the Gray word of h, the low rows'
+labels the Gray word of j read backwards for odd h, the per-D table vectors
+and the register vectors they are compared against."""
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+
+
+def gray_labels(x, ndig, d):
+    return O.labels(x, ndig + 1, d) if ndig > 0 else np.zeros(0, dtype=np.int32)
+
+
+def table_model(a, d, marginal, k):
+    """(max value, smallest Gray index) computed the way the kernel does."""
+    R, C = a.shape
+    F = R - 1
+    base = 2 if d <= 2 else d
+    B = base ** k
+    nh = F - k
+    K = int(np.abs(a[:, 0]).sum()) if marginal else 0
+    tot = a.sum(axis=0)
+    # table: vectors per low labeling j (Gray order)
+    table = []
+    for j in range(B):
+        lab = gray_labels(j, k, d)
+        if d == 1:
+            L = sum(((1 if lab[i] else -1) * a[i] for i in range(k)), np.zeros(C, dtype=np.int64))
+            table.append([-L])
+        else:
+            Ls = [sum((a[i] for i in range(k) if lab[i] == m), np.zeros(C, dtype=np.int64)) for m in range(3)]
+            if d == 2:
+                table.append([-Ls[1], tot - Ls[1]])
+            else:
+                table.append([-Ls[1], -Ls[2], tot - Ls[1] - Ls[2]])
+    best, bestN = None, None
+    for h in range(base ** nh):
+        lab = gray_labels(h, nh, d)
+        if d == 1:
+            H = a[R - 1].copy()
+            if marginal:
+                H[0] += K
+            for t in range(nh):
+                H += (1 if lab[t] else -1) * a[k + t]
+            regs = [H]
+        else:
+            Hm = [sum((a[k + t] for t in range(nh) if lab[t] == m), np.zeros(C, dtype=np.int64))
+                  for m in range(3)]
+            regs = [Hm[1], Hm[1]] if d == 2 else [Hm[1], Hm[2], Hm[1] + Hm[2]]
+        for jj in range(B):
+            je = B - 1 - jj if h & 1 else jj
+            v = sum(int(np.abs(r - e).sum()) for r, e in zip(regs, table[je])) - K
+            N = h * B + jj
+            if best is None or v > best or (v == best and N < bestN):
+                best, bestN = v, N
+    return best, bestN
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_table_decomposition_matches_oracle(seed):
+    rng = np.random.default_rng(seed)
+    d = [1, 2, 3][seed % 3]
+    marginal = d == 1 and seed % 2 == 1
+    R = int(rng.integers(2, {1: 10, 2: 10, 3: 7}[d]))
+    C = int(rng.integers(1, 6))
+    a = rng.integers(-4, 5, size=(R, C)).astype(np.int64)
+    k = int(rng.integers(0, R))       # 0 .. F low rows
+    assert table_model(a, d, marginal, k) == O.enumerate_max(a, d, marginal, nthreads=1)
