@@ -145,6 +145,21 @@ ld_status ld_solve_reduced(const int64_t *mtx_as_vec, int32_t rows, int32_t cols
                            int32_t marginal, const ld_options *opt, ld_result *res,
                            int32_t *strategy);
 
+/* No counterpart in the reference.  The same solve as ld_solve_reduced for
+ * callers that must not allocate GPU memory (cudaMalloc/cudaFree can
+ * synchronize the device, and fail once another framework in the process
+ * holds nearly all of its memory): all device working memory is one 64 KiB
+ * file-scope __device__ array, reserved on every GPU that loads the library.
+ * Host matrix in, host result out; `stream` may be NULL.  Limits: d <= 3,
+ * <= 63 rows, <= 64 columns (<= 128 when every partial column sum fits in 8
+ * bits), column sums within 32 bits; larger inputs get LD_ERR_LIMIT.  The
+ * first call on a device looks up the array's address (make it before any
+ * stream capture on that device).  Calls share the array and are serialised
+ * by a host lock; GPU work of two calls must not overlap.  kernel_ms is 0. */
+ld_status ld_solve_reduced_noalloc(const int64_t *mtx_as_vec, int32_t rows, int32_t cols,
+                                   int32_t d, int32_t marginal, int32_t device, void *stream,
+                                   ld_result *res, int32_t *strategy);
+
 /* Labels of rows 0..rows-2 for a Gray index (the BRGC word of L_CUDA.cu:61-63,
  * the d-ary reflected word of L_CUDA.cu:204-206). */
 ld_status ld_gray_labels(uint64_t index, int32_t rows, int32_t d, int32_t *labels);

@@ -71,6 +71,8 @@ SIGNATURES = [
     ("ld_problem_solve", C.c_int, [_P, C.POINTER(Options), C.POINTER(Result)]),
     ("ld_solve_reduced", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options),
                                    C.POINTER(Result), _I32P]),
+    ("ld_solve_reduced_noalloc", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                           C.c_void_p, C.POINTER(Result), _I32P]),
     ("ld_gray_labels", C.c_int, [C.c_uint64, C.c_int32, C.c_int32, _I32P]),
     ("ld_problem_report", C.c_int, [_P, C.POINTER(Result), _I32P, C.c_int32, _I32P, C.c_char_p, C.c_size_t]),
     ("ld_plan_create", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options), C.POINTER(_P)]),
@@ -154,6 +156,20 @@ def solve_reduced(a, d: int, marginal: bool = False, opts: Options | None = None
     _check(lib().ld_solve_reduced(a.ctypes.data_as(_I64P), r, c, d, int(marginal),
                                   C.byref(opts) if opts is not None else None, C.byref(res),
                                   labels.ctypes.data_as(_I32P)))
+    return _solution(res, labels[: max(r - 1, 0)])
+
+
+def solve_reduced_noalloc(a, d: int, marginal: bool = False, device: int = 0, stream: int = 0) -> Solution:
+    """ld_solve_reduced without any device allocation (its working memory is a
+    fixed 64 KiB device array inside the library); for callers that must not
+    allocate GPU memory.  d <= 3, <= 64 columns (128 with 8-bit sums)."""
+    a = _as_i64(a)
+    r, c = a.shape
+    labels = np.zeros(max(r - 1, 1), dtype=np.int32)
+    res = Result()
+    _check(lib().ld_solve_reduced_noalloc(a.ctypes.data_as(_I64P), r, c, d, int(marginal), device,
+                                          C.c_void_p(stream or None), C.byref(res),
+                                          labels.ctypes.data_as(_I32P)))
     return _solution(res, labels[: max(r - 1, 0)])
 
 
