@@ -193,6 +193,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   args.A = (const uint32_t*)(scratch + kA);
   args.tot = (const uint32_t*)(scratch + kTot);
   args.hinit = (const uint32_t*)(scratch + kH0);
+  args.tbias = nullptr;
   args.R = R; args.k = k; args.B = B; args.fw = fw;
   args.walk_len = walk_len; args.walk_begin = 0; args.walk_end = walks;
   args.value_offset = offset;

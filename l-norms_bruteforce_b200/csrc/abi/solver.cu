@@ -64,42 +64,105 @@ Bounds compute_bounds(const int64_t* a, int R, int C, int marginal) {
 
 struct Choice {
   int kind = LD_KERNEL_WIDE;
-  int D = 0, W = 0, PK = 0;          // table
-  int PC = 0, multi = 0, i64 = 0;    // wide
+  int D = 0, WB = 0, WA = 0, WT = 0, k = 0;   // table: int32 words, int8x4 words, padded, low rows
+  std::vector<int> order;                     // table: column of each lane (wide first)
+  int PC = 0, multi = 0, i64 = 0;             // wide
   int lane_bits = 0;
 };
 
 int round4(int x) { return (x + 3) & ~3; }
 
-ld_status choose_kernel(int R, int C, int d, int marginal, const Bounds& b, const ld_options& o,
-                        Choice* ch) {
+unsigned long long ipow(unsigned long long b, int e) {
+  unsigned long long r = 1;
+  for (int i = 0; i < e; ++i) r *= b;
+  return r;
+}
+
+// Table-kernel configuration for a given number of low rows k: which columns
+// can live in 8-bit lanes.  For d = 1 the two operands of each absolute
+// difference are the high rows' partial sum (with the fixed row) and the low
+// rows' partial sum, so each only needs its own part to fit 8 bits; for LM,
+// column 0 carries the shift K split the same way (K_H + K_L).  For d >= 2 a
+// table vector holds the column total minus low rows, so a column is narrow
+// when its full bound fits.  Returns false if no instance exists.
+bool table_config(const int64_t* a, int R, int C, int d, int marginal, int k, int force_bits,
+                  Choice* ch) {
+  std::vector<int> wide, narrow;
+  for (int l = 0; l < C; ++l) {
+    long long hb = 0, lb = 0;
+    for (int i = 0; i < R; ++i) {
+      const int64_t v = a[(size_t)i * C + l];
+      const long long av = v < 0 ? -(long long)v : (long long)v;
+      if (i < k) lb += av; else hb += av;
+    }
+    bool nar;
+    if (d == 1) nar = (marginal && l == 0) ? (2 * hb <= 127 && 2 * lb <= 128) : (hb <= 127 && lb <= 127);
+    else nar = hb + lb <= 127;
+    if (force_bits == 32) nar = false;
+    (nar ? narrow : wide).push_back(l);
+  }
+  if (force_bits == 8 && !wide.empty()) return false;
+  int WB = (int)wide.size(), WA = ((int)narrow.size() + 3) / 4;
+  if (d >= 2 && WB > 0 && WA > 0) {             // no mixed instances for d >= 2
+    if (force_bits == 8) return false;
+    wide.insert(wide.end(), narrow.begin(), narrow.end());
+    narrow.clear();
+    WB = C; WA = 0;
+  }
+  if (!ld::table_kernel_mixed_ptr(d, WB, WA)) {
+    if (force_bits == 8 || C > 64 || !ld::table_kernel_mixed_ptr(d, C, 0)) return false;
+    wide.clear();
+    for (int l = 0; l < C; ++l) wide.push_back(l);
+    narrow.clear();
+    WB = C; WA = 0;
+  }
+  ch->kind = LD_KERNEL_TABLE;
+  ch->D = d; ch->WB = WB; ch->WA = WA; ch->WT = round4(WB + WA); ch->k = k;
+  ch->order = wide;
+  ch->order.insert(ch->order.end(), narrow.begin(), narrow.end());
+  ch->lane_bits = WB > 0 ? 32 : 8;
+  return true;
+}
+
+// Pick the kernel and, for the table kernel, the low-row count minimizing
+// an estimate of the solve time: labelings x (words per labeling + the
+// amortized cost of a high-row step) / threads that have work.
+ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, const Bounds& b,
+                        const ld_options& o, unsigned long long full_threads, Choice* ch) {
   if (b.overflow) return ld_fail(LD_ERR_LIMIT, "matrix entries too large: column sums exceed 2^61");
   const long long maxabs = std::max(b.colbound, marginal ? 2 * b.K : 0LL);
   const long long vmax = b.total + (marginal ? b.K : 0LL);
   const bool fits32 = vmax <= (long long)INT32_MAX && maxabs <= (long long)INT32_MAX;
-  if (o.kernel != LD_KERNEL_WIDE && d <= 3 && o.lane_bits != 64) {
-    const int cand[2] = {4, 1};
-    for (int pk : cand) {
-      const int bits = 32 / pk;
-      if (o.lane_bits && o.lane_bits != bits) continue;
-      const long long lim = pk == 4 ? 127 : (long long)INT32_MAX;
-      if (maxabs > lim || !fits32) continue;
-      const int W = round4((C + pk - 1) / pk);
-      const int wmax = pk == 4 ? 32 : (d == 1 ? 64 : d == 2 ? 48 : 32);
-      if (W > wmax) continue;
-      ch->kind = LD_KERNEL_TABLE; ch->D = d; ch->W = W; ch->PK = pk; ch->lane_bits = bits;
-      return LD_OK;
+  if (o.lane_bits && o.lane_bits != 8 && o.lane_bits != 32 && o.lane_bits != 64)
+    return ld_fail(LD_ERR_ARG, "lane width %d is not 8, 32 or 64", o.lane_bits);
+  if (o.kernel != LD_KERNEL_WIDE && d <= 3 && o.lane_bits != 64 && fits32) {
+    const int base = d <= 2 ? 2 : d, F = R - 1;
+    double best_t = 0;
+    bool found = false;
+    for (int k = 0; k <= F; ++k) {
+      const unsigned long long B = ipow(base, k);
+      if (B > 1024) break;
+      if (o.low_rows >= 0 && k != std::min(o.low_rows, F)) continue;
+      Choice c;
+      if (!table_config(a, R, C, d, marginal, k, o.lane_bits, &c)) continue;
+      const int NW = d * c.WT;
+      if (B * (unsigned long long)NW > (o.low_rows >= 0 ? 16384ull : 8192ull)) continue;
+      const double words = (double)d * (c.WB + c.WA);
+      const double per_lab = words + (2.0 * words + 40.0) / (double)B;
+      const double highs = (double)ipow(base, F - k);
+      const double t = per_lab / std::min(highs, (double)full_threads);
+      if (!found || t < best_t * 0.999) { best_t = t; *ch = c; found = true; }
     }
+    if (found) return LD_OK;
     if (o.kernel == LD_KERNEL_TABLE)
       return ld_fail(LD_ERR_ARG, "the table kernel cannot take this matrix (d=%d, %d columns)", d, C);
   }
+  if (o.kernel == LD_KERNEL_TABLE)
+    return ld_fail(LD_ERR_ARG, "the table kernel cannot take this matrix (d=%d, %d columns)", d, C);
+  if (o.lane_bits == 8) return ld_fail(LD_ERR_ARG, "8-bit lanes need the table kernel");
   ch->kind = LD_KERNEL_WIDE;
   ch->i64 = (!fits32 || o.lane_bits == 64) ? 1 : 0;
   ch->lane_bits = ch->i64 ? 64 : 32;
-  if (o.lane_bits == 8)
-    return ld_fail(LD_ERR_ARG, "8-bit lanes need the table kernel");
-  if (o.lane_bits && o.lane_bits != 32 && o.lane_bits != 64)
-    return ld_fail(LD_ERR_ARG, "lane width %d is not 8, 32 or 64", o.lane_bits);
   int pc = 1;
   while (pc * 32 < C) pc *= 2;
   ch->PC = pc;
@@ -107,25 +170,17 @@ ld_status choose_kernel(int R, int C, int d, int marginal, const Bounds& b, cons
   return LD_OK;
 }
 
-uint32_t pack_word(const int64_t* v, int n, int pk) {
-  uint32_t w = 0;
-  const int bits = 32 / pk;
-  const uint32_t mask = bits == 32 ? 0xffffffffu : ((1u << bits) - 1u);
-  for (int q = 0; q < pk && q < n; ++q) w |= ((uint32_t)(int32_t)v[q] & mask) << (q * bits);
-  return w;
-}
-
-void pack_row(const int64_t* row, int C, int W, int pk, uint32_t* out) {
-  for (int w = 0; w < W; ++w) {
-    const int c0 = w * pk;
-    out[w] = c0 < C ? pack_word(row + c0, std::min(pk, C - c0), pk) : 0u;
-  }
-}
-
-unsigned long long ipow(unsigned long long b, int e) {
-  unsigned long long r = 1;
-  for (int i = 0; i < e; ++i) r *= b;
-  return r;
+// Pack one row into the kernel's words: WB int32 lanes (columns order[0..WB)),
+// then WA words of four int8 lanes (the following columns), zero padded to WT.
+void pack_row(const int64_t* row, const Choice& ch, uint32_t* out) {
+  const int n = (int)ch.order.size();
+  for (int w = 0; w < ch.WT; ++w) out[w] = 0u;
+  for (int w = 0; w < ch.WB; ++w) out[w] = (uint32_t)(int32_t)row[ch.order[w]];
+  for (int q = 0; q < ch.WA; ++q)
+    for (int c = 0; c < 4; ++c) {
+      const int p = ch.WB + 4 * q + c;
+      if (p < n) out[ch.WB + q] |= ((uint32_t)(int32_t)row[ch.order[p]] & 0xffu) << (8 * c);
+    }
 }
 
 struct DeviceInfo {
@@ -217,7 +272,7 @@ std::mutex g_ws_mu[64];
 Resources g_ws[64];
 
 constexpr size_t kOffCounter = 0, kOffGvalue = 8, kOffResult = 16;
-constexpr size_t kOffTot = 256, kOffH0 = 512, kOffA = 768;
+constexpr size_t kOffTot = 256, kOffH0 = 512, kOffTb = 768, kOffA = 1024;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -301,25 +356,21 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
   p->R = R; p->C = C; p->d = d; p->marginal = marginal;
   p->total = total;
   p->bounds = compute_bounds(a, R, C, marginal);
-  st = choose_kernel(R, C, d, marginal, p->bounds, o, &p->ch);
+  st = choose_kernel(a, R, C, d, marginal, p->bounds, o, (unsigned long long)di.sms * 4 * 128, &p->ch);
   if (st != LD_OK) { delete p; return st; }
 
   const int base = d <= 2 ? 2 : d;
   const int F = R - 1;
   std::vector<char> image;
   if (p->ch.kind == LD_KERNEL_TABLE) {
-    const int D = p->ch.D, W = p->ch.W, PK = p->ch.PK, NW = D * W;
-    p->kfn = ld::table_kernel_ptr(D, W, PK);
-    if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no table kernel for D=%d W=%d PK=%d", D, W, PK); }
-    // low rows: largest k with base^k <= 1024 and a table of at most 32 KB
-    const int maxB = std::min(1024, 8192 / NW);
-    int k = 0;
-    while (k < F && ipow(base, k + 1) <= (unsigned long long)maxB) ++k;
-    if (o.low_rows >= 0 && o.low_rows <= F && ipow(base, o.low_rows) * NW <= 16384ull) k = o.low_rows;
+    const int D = p->ch.D, WT = p->ch.WT;
+    p->kfn = ld::table_kernel_mixed_ptr(D, p->ch.WB, p->ch.WA);
+    if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no table kernel for D=%d WB=%d WA=%d", D, p->ch.WB, p->ch.WA); }
+    const int k = p->ch.k;
     p->k = k;
     p->B = (int)ipow(base, k);
     p->tpb = ld::kTableThreads;
-    p->smem = (size_t)ld::table_smem_words(D, W, R, p->B) * sizeof(uint32_t);
+    p->smem = (size_t)ld::table_smem_words(D, WT, R, p->B) * sizeof(uint32_t);
     if (cudaFuncSetAttribute(p->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem) != cudaSuccess) {
       delete p; return ld_fail(LD_ERR_CUDA, "cannot reserve %zu bytes of shared memory", p->smem);
     }
@@ -341,20 +392,30 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     const unsigned long long want = (mine + p->tpb - 1) / p->tpb;
     p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * bps, std::max(1ull, want));
     if (o.blocks > 0) p->blocks = o.blocks;
-    // upload image: header | totals | initial H | packed rows
-    std::vector<int64_t> tot(C, 0), h0(C, 0);
+    // upload image: header | totals | initial H | table bias | packed rows
+    std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
     for (int i = 0; i < R; ++i)
       for (int l = 0; l < C; ++l) tot[l] += a[(size_t)i * C + l];
     if (D == 1) {
       for (int l = 0; l < C; ++l) h0[l] = a[(size_t)(R - 1) * C + l];
-      if (marginal) { h0[0] += p->bounds.K; p->value_offset = p->bounds.K; }
+      if (marginal) {
+        long long kl = 0, kh = 0;   // the low rows' and the other rows' share of K
+        for (int i = 0; i < R; ++i) {
+          const int64_t v = a[(size_t)i * C];
+          (i < k ? kl : kh) += v < 0 ? -(long long)v : (long long)v;
+        }
+        h0[0] += kh;
+        tb[0] = -kl;
+        p->value_offset = kh + kl;
+      }
     }
-    p->upload_bytes = kOffA + (size_t)R * W * 4;
+    p->upload_bytes = kOffA + (size_t)R * WT * 4;
     image.assign(p->upload_bytes, 0);
-    pack_row(tot.data(), C, W, PK, (uint32_t*)(image.data() + kOffTot));
-    pack_row(h0.data(), C, W, PK, (uint32_t*)(image.data() + kOffH0));
+    pack_row(tot.data(), p->ch, (uint32_t*)(image.data() + kOffTot));
+    pack_row(h0.data(), p->ch, (uint32_t*)(image.data() + kOffH0));
+    pack_row(tb.data(), p->ch, (uint32_t*)(image.data() + kOffTb));
     for (int i = 0; i < R; ++i)
-      pack_row(a + (size_t)i * C, C, W, PK, (uint32_t*)(image.data() + kOffA) + (size_t)i * W);
+      pack_row(a + (size_t)i * C, p->ch, (uint32_t*)(image.data() + kOffA) + (size_t)i * WT);
   } else {
     p->kfn = ld::wide_kernel_ptr(p->ch.i64, p->ch.PC, p->ch.multi);
     if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no wide kernel for PC=%d", p->ch.PC); }
@@ -410,6 +471,7 @@ static ld_status plan_enqueue(ld_plan* p) {
     args.A = (const uint32_t*)(base_ptr + kOffA);
     args.tot = (const uint32_t*)(base_ptr + kOffTot);
     args.hinit = (const uint32_t*)(base_ptr + kOffH0);
+    args.tbias = (const uint32_t*)(base_ptr + kOffTb);
     args.R = p->R; args.k = p->k; args.B = p->B; args.fw = p->fw;
     args.walk_len = p->walk_len; args.walk_begin = p->walk_begin; args.walk_end = p->walk_end;
     args.value_offset = p->value_offset;
@@ -496,8 +558,8 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (!p || !buf) return ld_fail(LD_ERR_ARG, "null argument");
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
-             "table D=%d W=%d PK=%d (%d-bit lanes) k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d smem=%zu",
-             p->ch.D, p->ch.W, p->ch.PK, p->ch.lane_bits, p->k, p->B, p->fw,
+             "table D=%d int32 words=%d int8x4 words=%d k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d smem=%zu",
+             p->ch.D, p->ch.WB, p->ch.WA, p->k, p->B, p->fw,
              (unsigned long long)p->walks, p->blocks, p->tpb, p->smem);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d", p->ch.PC, p->ch.multi,

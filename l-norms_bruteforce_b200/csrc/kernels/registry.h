@@ -2,11 +2,27 @@
 #pragma once
 
 namespace ld {
-// table_kernel<D, W, PK> for D in {1,2,3}, W in {4,8,...,32}, PK in {1,2,4};
-// nullptr when not instantiated.
+
+// table_kernel<D, WB, WA> by (D, WB, WA): D in 1..3, WB int32 words (0..64),
+// WA int8x4 words (0..32).  Instances:
+//   D = 1: WB <= 4 with WA <= 16 (mixed), WA <= 32 with WB = 0, WB <= 64 with WA = 0
+//   D = 2: WB <= 48 with WA = 0, WA <= 32 with WB = 0
+//   D = 3: WB <= 32 with WA = 0, WA <= 32 with WB = 0
+using TableKernelTab = const void* [4][65][33];
+void table_register_d1_mix(TableKernelTab& t);
+void table_register_d1_p8(TableKernelTab& t);
+void table_register_d1_p32a(TableKernelTab& t);
+void table_register_d1_p32b(TableKernelTab& t);
+void table_register_d2(TableKernelTab& t);
+void table_register_d3(TableKernelTab& t);
+
+// nullptr when not instantiated
+const void* table_kernel_mixed_ptr(int D, int WB, int WA);
+// all columns in one lane width: PK = 1 (int32, W words) or 4 (int8x4, W words)
 const void* table_kernel_ptr(int D, int W, int PK);
 // wide_kernel<IT, PC, MULTI>, PC in {1,2,4,...,128}
 const void* wide_kernel_ptr(int i64, int PC, int multi);
+
 }  // namespace ld
 
 #define LD_WIDE_MAXD 10

@@ -1,23 +1,8 @@
-// table_kernel instances for D = 2: int32 lanes (PK = 1) for W = 4..48 words,
-// int8x4 lanes (PK = 4) for W = 4..32 words.
-#include <utility>
-
-#include "registry.h"
-#include "table_kernel.cuh"
-
+// table_kernel<2, WB, 0> for WB = 1..48 and table_kernel<2, 0, WA> for WA = 1..32.
+#include "table_inst.cuh"
 namespace ld {
-
-template <int PK, int... Ws>
-static const void* pick_d2(int W, std::integer_sequence<int, Ws...>) {
-  const void* r = nullptr;
-  ((W == (Ws + 1) * 4 ? (r = (const void*)&table_kernel<2, (Ws + 1) * 4, PK>, 0) : 0), ...);
-  return r;
+void table_register_d2(TableKernelTab& t) {
+  inst::fill_wb<2, 0, 1>(t, std::make_integer_sequence<int, 48>{});
+  inst::fill_wa<2, 0, 1>(t, std::make_integer_sequence<int, 32>{});
 }
-
-const void* table_kernel_ptr_d2(int W, int PK) {
-  if (PK == 1) return pick_d2<1>(W, std::make_integer_sequence<int, 12>{});
-  if (PK == 4) return pick_d2<4>(W, std::make_integer_sequence<int, 8>{});
-  return nullptr;
-}
-
 }  // namespace ld

@@ -1,23 +1,8 @@
-// table_kernel instances for D = 3: int32 lanes (PK = 1) for W = 4..32 words,
-// int8x4 lanes (PK = 4) for W = 4..32 words.
-#include <utility>
-
-#include "registry.h"
-#include "table_kernel.cuh"
-
+// table_kernel<3, WB, 0> for WB = 1..32 and table_kernel<3, 0, WA> for WA = 1..32.
+#include "table_inst.cuh"
 namespace ld {
-
-template <int PK, int... Ws>
-static const void* pick_d3(int W, std::integer_sequence<int, Ws...>) {
-  const void* r = nullptr;
-  ((W == (Ws + 1) * 4 ? (r = (const void*)&table_kernel<3, (Ws + 1) * 4, PK>, 0) : 0), ...);
-  return r;
+void table_register_d3(TableKernelTab& t) {
+  inst::fill_wb<3, 0, 1>(t, std::make_integer_sequence<int, 32>{});
+  inst::fill_wa<3, 0, 1>(t, std::make_integer_sequence<int, 32>{});
 }
-
-const void* table_kernel_ptr_d3(int W, int PK) {
-  if (PK == 1) return pick_d3<1>(W, std::make_integer_sequence<int, 8>{});
-  if (PK == 4) return pick_d3<4>(W, std::make_integer_sequence<int, 8>{});
-  return nullptr;
-}
-
 }  // namespace ld

@@ -11,32 +11,41 @@
 // Each block tabulates, once, the low rows' contribution to the message
 // column sums for all B low labelings (Gray order, shared memory).  Each
 // thread keeps the high rows' column sums H in registers, walks h in Gray
-// order (one row changes per step: one packed add or subtract of a row
-// staged in shared memory), and for every h evaluates all B labelings as
-//     sum over message vectors and columns of |H + L_j|
-// with one packed absolute-difference-accumulate per column word against
-// the tabulated entry (a warp-uniform broadcast read).  With PK columns per
-// 32-bit word (int8x4 / int16x2 / int32 lanes, chosen by the host from an
-// exact bound) one instruction covers PK columns.
+// order (one row changes per step: one add or subtract of a row staged in
+// shared memory), and for every h evaluates all B labelings as
+//     sum over table vectors and columns of |H - T_j|
+// with one absolute-difference-accumulate instruction per column word
+// against the tabulated entry (a warp-uniform broadcast read).
 //
-// Message vectors per labeling (NV = D):
-//   D = 1 (L_1 / LM): s = A_fixed + sum s_i A_i;          table: -L
+// Column words.  A vector has WB words holding one column each as a 32-bit
+// lane (`__sad`), then WA words holding four columns each as signed 8-bit
+// lanes (`vabsdiff4`, the same issue cost as one `__sad`).  The host puts a
+// column in an 8-bit lane only when every value either operand can take
+// fits in 8 bits (the instruction forms |a - b| at full width), so the lane
+// arithmetic is exact.  Rows and table vectors are padded to WT words, a
+// multiple of 4, for 16-byte shared-memory loads.
+//
+// Message vectors per labeling (D):
+//   D = 1 (L_1 / LM): s = A_fixed + sum s_i A_i;          table: tb - L
 //   D = 2 (L_2):      s1 = rows labelled 1, s0 = T - s1;   table: -L1, T-L1
 //     both table vectors are compared against the same register vector H
 //     (|H + L1| + |H - (T - L1)|);
 //   D = 3 (L_3):      s1, s2, s0 = T - s1 - s2;            table: -L1, -L2, T-L1-L2
 //     with registers H1, H2 and H1+H2.
-// LM enters as L_1 with column 0 shifted by K = sum_i |A_i0| (host side),
-// which makes that column's term equal to its signed sum plus K.
+// LM enters as L_1 with column 0 shifted by K = sum_i |A_i0|: K_H (the
+// high and fixed rows' share) is added to H's column 0 and K_L (the low
+// rows' share) is subtracted through the table bias tb, so that column's
+// term is its signed sum plus K; K is subtracted from the result.
 #pragma once
 #include "common.cuh"
 
 namespace ld {
 
 struct TableArgs {
-  const uint32_t* A;        // R x W packed rows; row R-1 is the fixed row
-  const uint32_t* tot;      // W words: column totals over all rows (D >= 2)
-  const uint32_t* hinit;    // W words: H before any high row (D = 1: fixed row)
+  const uint32_t* A;        // R x WT packed rows; row R-1 is the fixed row
+  const uint32_t* tot;      // WT words: column totals over all rows (D >= 2)
+  const uint32_t* hinit;    // WT words: H before any high row (D = 1: fixed row)
+  const uint32_t* tbias;    // WT words added to every D = 1 table vector, or null
   int R;                    // reduced rows
   int k;                    // low rows (tabulated)
   int B;                    // d^k
@@ -49,71 +58,88 @@ struct TableArgs {
 
 constexpr int kTableThreads = 128;
 
-__host__ __device__ constexpr int table_words(int D, int W) { return D * W; }
-// register words of H: one vector for D <= 2, three for D = 3
-__host__ __device__ constexpr int reg_words(int D, int W) { return D == 3 ? 3 * W : W; }
-// register word that table word q is compared with
-template <int D, int W>
-__device__ __forceinline__ constexpr int hword(int q) { return D == 2 ? q % W : q; }
+// padded words of one row / table vector
+__host__ __device__ constexpr int table_row_words(int WB, int WA) { return (WB + WA + 3) & ~3; }
 
-// Shared memory: packed rows, totals, initial H, then the table (16-byte
-// aligned).
+// Shared memory (32-bit words): packed rows, totals, initial H, table bias,
+// then the table (16-byte aligned).  W is the padded row width.
 __host__ __device__ inline int table_smem_words(int D, int W, int R, int B) {
-  int head = R * W + 2 * W;
+  int head = R * W + 3 * W;
   head = (head + 3) & ~3;
   return head + B * D * W;
 }
 
-template <int D, int W, int PK>
-__device__ __forceinline__ void add_row(uint32_t* H, const uint32_t* row, int vec) {
-  using L = Lanes<PK>;
-#pragma unroll
-  for (int w = 0; w < W; ++w) H[vec * W + w] = L::add(H[vec * W + w], row[w]);
+template <int D, int WB, int WA>
+struct Shape {
+  static constexpr int WV = WB + WA;                  // computed words per vector
+  static constexpr int WT = (WV + 3) & ~3;            // padded words per vector
+  static constexpr int NW = D * WT;                   // words per table entry
+  static constexpr int NR = D == 3 ? 3 : 1;           // register vectors
+};
+
+template <int WB>
+__device__ __forceinline__ uint32_t wadd(int w, uint32_t a, uint32_t b) {
+  return w < WB ? Lanes<1>::add(a, b) : Lanes<4>::add(a, b);
+}
+template <int WB>
+__device__ __forceinline__ uint32_t wsub(int w, uint32_t a, uint32_t b) {
+  return w < WB ? Lanes<1>::sub(a, b) : Lanes<4>::sub(a, b);
+}
+template <int WB>
+__device__ __forceinline__ uint32_t wsad(int w, uint32_t a, uint32_t b, uint32_t c) {
+  return w < WB ? Lanes<1>::sad(a, b, c) : Lanes<4>::sad(a, b, c);
 }
 
-template <int D, int W, int PK>
-__device__ __forceinline__ void sub_row(uint32_t* H, const uint32_t* row, int vec) {
-  using L = Lanes<PK>;
+template <int D, int WB, int WA>
+__device__ __forceinline__ void add_row(uint32_t* H, const uint32_t* row, int vec) {
+  constexpr int WV = Shape<D, WB, WA>::WV;
 #pragma unroll
-  for (int w = 0; w < W; ++w) H[vec * W + w] = L::sub(H[vec * W + w], row[w]);
+  for (int w = 0; w < WV; ++w) H[vec * WV + w] = wadd<WB>(w, H[vec * WV + w], row[w]);
+}
+
+template <int D, int WB, int WA>
+__device__ __forceinline__ void sub_row(uint32_t* H, const uint32_t* row, int vec) {
+  constexpr int WV = Shape<D, WB, WA>::WV;
+#pragma unroll
+  for (int w = 0; w < WV; ++w) H[vec * WV + w] = wsub<WB>(w, H[vec * WV + w], row[w]);
 }
 
 // Move high row r from label a to label b.
-template <int D, int W, int PK>
+template <int D, int WB, int WA>
 __device__ __forceinline__ void move_row(uint32_t* H, const uint32_t* row, int a, int b) {
   if (D == 1) {  // sign a -> b: add or subtract 2 * row (as two steps, each in range)
-    if (b) { add_row<D, W, PK>(H, row, 0); add_row<D, W, PK>(H, row, 0); }
-    else   { sub_row<D, W, PK>(H, row, 0); sub_row<D, W, PK>(H, row, 0); }
+    if (b) { add_row<D, WB, WA>(H, row, 0); add_row<D, WB, WA>(H, row, 0); }
+    else   { sub_row<D, WB, WA>(H, row, 0); sub_row<D, WB, WA>(H, row, 0); }
   } else if (D == 2) {
-    if (b) add_row<D, W, PK>(H, row, 0); else sub_row<D, W, PK>(H, row, 0);
+    if (b) add_row<D, WB, WA>(H, row, 0); else sub_row<D, WB, WA>(H, row, 0);
   } else {
-    if (a == 1) sub_row<D, W, PK>(H, row, 0);
-    if (a == 2) sub_row<D, W, PK>(H, row, 1);
-    if (b == 1) add_row<D, W, PK>(H, row, 0);
-    if (b == 2) add_row<D, W, PK>(H, row, 1);
-    if (a == 0 && b != 0) add_row<D, W, PK>(H, row, 2);
-    if (a != 0 && b == 0) sub_row<D, W, PK>(H, row, 2);
+    if (a == 1) sub_row<D, WB, WA>(H, row, 0);
+    if (a == 2) sub_row<D, WB, WA>(H, row, 1);
+    if (b == 1) add_row<D, WB, WA>(H, row, 0);
+    if (b == 2) add_row<D, WB, WA>(H, row, 1);
+    if (a == 0 && b != 0) add_row<D, WB, WA>(H, row, 2);
+    if (a != 0 && b == 0) sub_row<D, WB, WA>(H, row, 2);
   }
 }
 
 // H for high index h: initial vector plus every high row at its label.
-template <int D, int W, int PK>
+template <int D, int WB, int WA>
 __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const uint32_t* sH0,
                                           int k, int nh, unsigned long long h) {
-  constexpr int NV = D == 3 ? 3 : 1;
+  using S = Shape<D, WB, WA>;
 #pragma unroll
-  for (int w = 0; w < W; ++w) H[w] = sH0[w];
+  for (int w = 0; w < S::WV; ++w) H[w] = sH0[w];
 #pragma unroll
-  for (int v = 1; v < NV; ++v)
+  for (int v = 1; v < S::NR; ++v)
 #pragma unroll
-    for (int w = 0; w < W; ++w) H[v * W + w] = 0u;
+    for (int w = 0; w < S::WV; ++w) H[v * S::WV + w] = 0u;
   if (D <= 2) {
     const unsigned long long g = h ^ (h >> 1);
     for (int t = 0; t < nh; ++t) {
       const int lab = (int)((g >> t) & 1ull);
-      const uint32_t* row = sA + (k + t) * W;
-      if (D == 1) { if (lab) add_row<D, W, PK>(H, row, 0); else sub_row<D, W, PK>(H, row, 0); }
-      else if (lab) add_row<D, W, PK>(H, row, 0);
+      const uint32_t* row = sA + (k + t) * S::WT;
+      if (D == 1) { if (lab) add_row<D, WB, WA>(H, row, 0); else sub_row<D, WB, WA>(H, row, 0); }
+      else if (lab) add_row<D, WB, WA>(H, row, 0);
     }
   } else {
     unsigned long long q = h;
@@ -121,95 +147,112 @@ __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const
       const int r = (int)(q % 6ull);
       const int lab = r < 3 ? r : 5 - r;
       q /= 3ull;
-      const uint32_t* row = sA + (k + t) * W;
-      if (lab == 1) { add_row<D, W, PK>(H, row, 0); add_row<D, W, PK>(H, row, 2); }
-      else if (lab == 2) { add_row<D, W, PK>(H, row, 1); add_row<D, W, PK>(H, row, 2); }
+      const uint32_t* row = sA + (k + t) * S::WT;
+      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); add_row<D, WB, WA>(H, row, 2); }
+      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); add_row<D, WB, WA>(H, row, 2); }
+    }
+  }
+}
+
+// register word compared with table word q (q in [0, NW))
+template <int D, int WB, int WA>
+__device__ __forceinline__ constexpr int reg_of(int q) {
+  using S = Shape<D, WB, WA>;
+  return (D == 3 ? (q / S::WT) : 0) * S::WV + q % S::WT;
+}
+template <int D, int WB, int WA>
+__device__ __forceinline__ constexpr bool computed(int q) {
+  using S = Shape<D, WB, WA>;
+  return q % S::WT < S::WV;
+}
+
+// acc += |H - e| over the words of x (table words 4q .. 4q+3)
+template <int D, int WB, int WA>
+__device__ __forceinline__ void sad4(const uint32_t* H, const uint4& x, int q, uint32_t& a0, uint32_t& a1) {
+  using S = Shape<D, WB, WA>;
+  const uint32_t xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int tq = 4 * q + c;
+    if (computed<D, WB, WA>(tq)) {
+      uint32_t& acc = (c & 1) ? a1 : a0;
+      acc = wsad<WB>(tq % S::WT, H[reg_of<D, WB, WA>(tq)], xs[c], acc);
     }
   }
 }
 
 // Value of table entry e against H.
-template <int D, int W, int PK>
+template <int D, int WB, int WA>
 __device__ __forceinline__ int entry_value(const uint32_t* H, const uint32_t* e) {
-  using L = Lanes<PK>;
-  constexpr int NW = D * W;
+  using S = Shape<D, WB, WA>;
   const uint4* t = reinterpret_cast<const uint4*>(e);
   uint32_t a0 = 0u, a1 = 0u;
 #pragma unroll
-  for (int q = 0; q < NW / 4; ++q) {
-    const uint4 x = t[q];
-    a0 = L::sad(H[hword<D, W>(4 * q + 0)], x.x, a0);
-    a1 = L::sad(H[hword<D, W>(4 * q + 1)], x.y, a1);
-    a0 = L::sad(H[hword<D, W>(4 * q + 2)], x.z, a0);
-    a1 = L::sad(H[hword<D, W>(4 * q + 3)], x.w, a1);
-  }
+  for (int q = 0; q < S::NW / 4; ++q) sad4<D, WB, WA>(H, t[q], q, a0, a1);
   return (int)(a0 + a1);
 }
 
 // max over all B table entries
-template <int D, int W, int PK>
+template <int D, int WB, int WA>
 __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, int B) {
-  using L = Lanes<PK>;
-  constexpr int NW = D * W;
+  using S = Shape<D, WB, WA>;
   int m = INT_MIN;
   int j = 0;
   for (; j + 2 <= B; j += 2) {
-    const uint4* t0 = reinterpret_cast<const uint4*>(sT + j * NW);
-    const uint4* t1 = reinterpret_cast<const uint4*>(sT + (j + 1) * NW);
+    const uint4* t0 = reinterpret_cast<const uint4*>(sT + j * S::NW);
+    const uint4* t1 = reinterpret_cast<const uint4*>(sT + (j + 1) * S::NW);
     uint32_t a0 = 0u, a1 = 0u, b0 = 0u, b1 = 0u;
 #pragma unroll
-    for (int q = 0; q < NW / 4; ++q) {
+    for (int q = 0; q < S::NW / 4; ++q) {
       const uint4 x = t0[q];
       const uint4 y = t1[q];
-      const uint32_t h0 = H[hword<D, W>(4 * q + 0)], h1 = H[hword<D, W>(4 * q + 1)];
-      const uint32_t h2 = H[hword<D, W>(4 * q + 2)], h3 = H[hword<D, W>(4 * q + 3)];
-      a0 = L::sad(h0, x.x, a0);
-      b0 = L::sad(h0, y.x, b0);
-      a1 = L::sad(h1, x.y, a1);
-      b1 = L::sad(h1, y.y, b1);
-      a0 = L::sad(h2, x.z, a0);
-      b0 = L::sad(h2, y.z, b0);
-      a1 = L::sad(h3, x.w, a1);
-      b1 = L::sad(h3, y.w, b1);
+      sad4<D, WB, WA>(H, x, q, a0, a1);
+      sad4<D, WB, WA>(H, y, q, b0, b1);
     }
     m = max(m, max((int)(a0 + a1), (int)(b0 + b1)));
   }
-  if (j < B) m = max(m, entry_value<D, W, PK>(H, sT + j * NW));
+  if (j < B) m = max(m, entry_value<D, WB, WA>(H, sT + j * S::NW));
   return m;
 }
 
-template <int D, int W, int PK>
+template <int D, int WB, int WA>
 __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs args) {
-  constexpr int NW = D * W;
+  using S = Shape<D, WB, WA>;
+  constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
   extern __shared__ __align__(16) uint32_t smem[];
   const int R = args.R, k = args.k, B = args.B;
   const int nh = R - 1 - k;  // high rows
   uint32_t* sA = smem;
-  uint32_t* sTot = sA + R * W;
-  uint32_t* sH0 = sTot + W;
-  uint32_t* sT = smem + (((R * W + 2 * W) + 3) & ~3);
+  uint32_t* sTot = sA + R * WT;
+  uint32_t* sH0 = sTot + WT;
+  uint32_t* sTb = sH0 + WT;
+  uint32_t* sT = smem + (((R * WT + 3 * WT) + 3) & ~3);
 
-  for (int t = threadIdx.x; t < R * W; t += blockDim.x) sA[t] = args.A[t];
-  for (int t = threadIdx.x; t < W; t += blockDim.x) { sTot[t] = args.tot[t]; sH0[t] = args.hinit[t]; }
+  for (int t = threadIdx.x; t < R * WT; t += blockDim.x) sA[t] = args.A[t];
+  for (int t = threadIdx.x; t < WT; t += blockDim.x) {
+    sTot[t] = args.tot[t];
+    sH0[t] = args.hinit[t];
+    sTb[t] = args.tbias ? args.tbias[t] : 0u;
+  }
   __syncthreads();
 
   // Tabulate the low rows' partial sums for every low labeling j (Gray order).
   for (int j = threadIdx.x; j < B; j += blockDim.x) {
-    uint32_t L1[W], L2[W];
+    uint32_t L1[WV], L2[WV];
 #pragma unroll
-    for (int w = 0; w < W; ++w) { L1[w] = 0u; L2[w] = 0u; }
+    for (int w = 0; w < WV; ++w) { L1[w] = D == 1 ? sTb[w] : 0u; L2[w] = 0u; }
     if (D <= 2) {
       const unsigned g = (unsigned)j ^ ((unsigned)j >> 1);
       for (int i = 0; i < k; ++i) {
         const int lab = (g >> i) & 1u;
-        const uint32_t* row = sA + i * W;
+        const uint32_t* row = sA + i * WT;
         if (D == 1) {
-          // entry = -(sum s_i A_i): subtract rows labelled +1, add rows labelled -1
+          // entry = tb - sum s_i A_i: subtract rows labelled +1, add rows labelled -1
 #pragma unroll
-          for (int w = 0; w < W; ++w) L1[w] = lab ? Lanes<PK>::sub(L1[w], row[w]) : Lanes<PK>::add(L1[w], row[w]);
+          for (int w = 0; w < WV; ++w) L1[w] = lab ? wsub<WB>(w, L1[w], row[w]) : wadd<WB>(w, L1[w], row[w]);
         } else if (lab) {
 #pragma unroll
-          for (int w = 0; w < W; ++w) L1[w] = Lanes<PK>::add(L1[w], row[w]);
+          for (int w = 0; w < WV; ++w) L1[w] = wadd<WB>(w, L1[w], row[w]);
         }
       }
     } else {
@@ -218,32 +261,33 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
         const unsigned r = q % 6u;
         const int lab = r < 3u ? (int)r : 5 - (int)r;
         q /= 3u;
-        const uint32_t* row = sA + i * W;
+        const uint32_t* row = sA + i * WT;
         if (lab == 1) {
 #pragma unroll
-          for (int w = 0; w < W; ++w) L1[w] = Lanes<PK>::add(L1[w], row[w]);
+          for (int w = 0; w < WV; ++w) L1[w] = wadd<WB>(w, L1[w], row[w]);
         } else if (lab == 2) {
 #pragma unroll
-          for (int w = 0; w < W; ++w) L2[w] = Lanes<PK>::add(L2[w], row[w]);
+          for (int w = 0; w < WV; ++w) L2[w] = wadd<WB>(w, L2[w], row[w]);
         }
       }
     }
     uint32_t* e = sT + j * NW;
-    if (D == 1) {
 #pragma unroll
-      for (int w = 0; w < W; ++w) e[w] = L1[w];
-    } else if (D == 2) {
+    for (int w = 0; w < WT; ++w) {
+      if (w < WV) {
+        if (D == 1) {
+          e[w] = L1[w];
+        } else if (D == 2) {
+          e[w] = wsub<WB>(w, 0u, L1[w]);
+          e[WT + w] = wsub<WB>(w, sTot[w], L1[w]);
+        } else {
+          e[w] = wsub<WB>(w, 0u, L1[w]);
+          e[WT + w] = wsub<WB>(w, 0u, L2[w]);
+          e[2 * WT + w] = wsub<WB>(w, wsub<WB>(w, sTot[w], L1[w]), L2[w]);
+        }
+      } else {
 #pragma unroll
-      for (int w = 0; w < W; ++w) {
-        e[w] = Lanes<PK>::sub(0u, L1[w]);
-        e[W + w] = Lanes<PK>::sub(sTot[w], L1[w]);
-      }
-    } else {
-#pragma unroll
-      for (int w = 0; w < W; ++w) {
-        e[w] = Lanes<PK>::sub(0u, L1[w]);
-        e[W + w] = Lanes<PK>::sub(0u, L2[w]);
-        e[2 * W + w] = Lanes<PK>::sub(Lanes<PK>::sub(sTot[w], L1[w]), L2[w]);
+        for (int v = 0; v < D; ++v) e[v * WT + w] = 0u;
       }
     }
   }
@@ -254,12 +298,12 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
   const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long WL = args.walk_len;
-  uint32_t H[reg_words(D, W)];
+  uint32_t H[S::NR * WV];
   int best = INT_MIN;
   unsigned long long best_h = 0ull;
   for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += T) {
     const unsigned long long h0 = wk * WL;
-    seed_high<D, W, PK>(H, sA, sH0, k, nh, h0);
+    seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
     for (unsigned long long u = 0; u < WL; ++u) {
       if (u) {
         const unsigned long long h = h0 + u;
@@ -278,9 +322,9 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
           b = par ? 2 - c : c;
           a = par ? 3 - c : c - 1;
         }
-        move_row<D, W, PK>(H, sA + (k + i) * W, a, b);
+        move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
       }
-      const int m = scan_max<D, W, PK>(H, sT, B);
+      const int m = scan_max<D, WB, WA>(H, sT, B);
       if (m > best) { best = m; best_h = h0 + u; }
     }
   }
@@ -290,11 +334,11 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
   long long bv = LLONG_MIN;
   unsigned long long bn = ULLONG_MAX;
   if (best != INT_MIN) {
-    seed_high<D, W, PK>(H, sA, sH0, k, nh, best_h);
+    seed_high<D, WB, WA>(H, sA, sH0, k, nh, best_h);
     const bool rev = (best_h & 1ull) != 0ull;
     for (int jj = 0; jj < B; ++jj) {
       const int je = rev ? B - 1 - jj : jj;
-      if (entry_value<D, W, PK>(H, sT + je * NW) == best) {
+      if (entry_value<D, WB, WA>(H, sT + je * NW) == best) {
         bn = best_h * (unsigned long long)B + (unsigned long long)jj;
         break;
       }

@@ -1,17 +1,32 @@
-// wide_kernel instances and the kernel registry.
+// wide_kernel instances and the kernel lookup.
 #include "registry.h"
 #include "wide_kernel.cuh"
 
 namespace ld {
 
-const void* table_kernel_ptr_d1(int W, int PK);
-const void* table_kernel_ptr_d2(int W, int PK);
-const void* table_kernel_ptr_d3(int W, int PK);
+static const TableKernelTab& table_kernels() {
+  static TableKernelTab tab = {};
+  static bool init = [] {
+    table_register_d1_mix(tab);
+    table_register_d1_p8(tab);
+    table_register_d1_p32a(tab);
+    table_register_d1_p32b(tab);
+    table_register_d2(tab);
+    table_register_d3(tab);
+    return true;
+  }();
+  (void)init;
+  return tab;
+}
+
+const void* table_kernel_mixed_ptr(int D, int WB, int WA) {
+  if (D < 1 || D > 3 || WB < 0 || WB > 64 || WA < 0 || WA > 32) return nullptr;
+  return table_kernels()[D][WB][WA];
+}
 
 const void* table_kernel_ptr(int D, int W, int PK) {
-  if (D == 1) return table_kernel_ptr_d1(W, PK);
-  if (D == 2) return table_kernel_ptr_d2(W, PK);
-  if (D == 3) return table_kernel_ptr_d3(W, PK);
+  if (PK == 1) return table_kernel_mixed_ptr(D, W, 0);
+  if (PK == 4) return table_kernel_mixed_ptr(D, 0, W);
   return nullptr;
 }
 

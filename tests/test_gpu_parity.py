@@ -174,3 +174,36 @@ def test_full_size_witness_and_invariances(ld, workloads):
     parts = [ld.solve_reduced(a, 1, False, ld.options(shard_index=s, shard_count=4)) for s in range(4)]
     best = max((p.value, -p.gray_index) for p in parts)
     assert (best[0], -best[1]) == (base.value, base.gray_index)
+
+
+@pytest.mark.parametrize("seed", range(16))
+def test_mixed_lane_widths(ld, seed):
+    """d = 1 matrices whose columns split between 8-bit and 32-bit lanes
+    (most columns small, a few large), with and without marginals, over
+    several low-row counts."""
+    rng = np.random.default_rng(500 + seed)
+    r = int(rng.integers(8, 21))
+    c = int(rng.integers(3, 40))
+    a = rng.integers(-3, 4, size=(r, c)).astype(np.int64)
+    for col in rng.choice(c, size=int(rng.integers(1, min(c, 4) + 1)), replace=False):
+        a[:, col] = rng.integers(-90, 91, size=r)
+    marg = bool(seed % 2)
+    ref = O.enumerate_max(a, 1, marg)
+    for k in (-1, 0, 3, 7, r - 1):
+        plan = ld.Plan(a, 1, marg, ld.options(kernel=1, low_rows=k))
+        sol = plan.solve()
+        assert (sol.value, sol.gray_index) == ref, plan.describe()
+        plan.close()
+
+
+def test_config2_uses_mixed_lanes(ld, workloads):
+    inst = workloads.config2()
+    p = ld.Problem.from_matrix(inst.matrix, 1, "y", True)
+    plan = ld.Plan(p.reduced, 1, True)
+    desc = plan.describe()
+    assert "int8x4 words=0" not in desc, desc
+    sol = plan.solve()
+    golden = next(c for c in GOLDEN if c["name"] == inst.name)
+    assert f"LM is: {sol.value}" in golden["stdout"]
+    assert (sol.value, sol.gray_index) == (398, 3585128208)
+    plan.close()
