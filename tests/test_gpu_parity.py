@@ -189,7 +189,7 @@ def test_mixed_lane_widths(ld, seed):
         a[:, col] = rng.integers(-90, 91, size=r)
     marg = bool(seed % 2)
     ref = O.enumerate_max(a, 1, marg)
-    for k in (-1, 0, 3, 7, r - 1):
+    for k in (-1, 0, 3, 7, min(r - 1, 10)):
         plan = ld.Plan(a, 1, marg, ld.options(kernel=1, low_rows=k))
         sol = plan.solve()
         assert (sol.value, sol.gray_index) == ref, plan.describe()
