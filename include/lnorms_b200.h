@@ -160,6 +160,38 @@ ld_status ld_solve_reduced_noalloc(const int64_t *mtx_as_vec, int32_t rows, int3
                                    int32_t d, int32_t marginal, int32_t device, void *stream,
                                    ld_result *res, int32_t *strategy);
 
+/* ---------------------------------------------------------------------- */
+/* Pruned exact search (no counterpart in the reference: it speeds the      */
+/* enumeration of calc_Lnorm up without changing its answer).  Blocks of    */
+/* labelings whose exact integer upper bound (|prefix column sums| + the    */
+/* norm of the remaining rows, per message) is below the incumbent are      */
+/* skipped; ties are never skipped, so value and Gray index equal           */
+/* ld_solve_reduced's.  `incumbent_labels` (rows-1 labels, may be NULL) is  */
+/* a labeling whose value the host recomputes.  d <= 3 inside the table     */
+/* kernel's range; other inputs fall back to the plain enumeration          */
+/* (stats->pruned = 0).                                                     */
+typedef struct {
+    uint64_t walks_total, walks_kept;         /* top-row prefixes, and those not pruned */
+    uint64_t highs_total, highs_visited, highs_kept;  /* high indices (blocks of `block` labelings) */
+    uint64_t block;                           /* labelings per high index                */
+    int64_t incumbent;                        /* value of the incumbent (INT64_MIN: none) */
+    float bound_ms, scan_ms;                  /* device time of the two launches          */
+    int32_t pruned;                           /* 1: pruned kernels ran; 0: plain fallback */
+    int32_t low_rows, walk_rows;              /* rows tabulated / walked per prefix       */
+} ld_prune_stats;
+ld_status ld_solve_pruned(const int64_t *mtx_as_vec, int32_t rows, int32_t cols, int32_t d,
+                          int32_t marginal, const ld_options *opt, const int32_t *incumbent_labels,
+                          ld_result *res, int32_t *strategy, ld_prune_stats *stats);
+
+/* Single-row-move local search on the GPU (no counterpart in the reference):
+ * n starting labelings (n x (rows-1) labels) are improved by steepest-ascent
+ * moves of one row's label until no move gains (or max_rounds, 0 = 4*rows);
+ * values[n] and labels[n x (rows-1)] receive the results.  d <= 3,
+ * <= 64 rows, <= 128 columns. */
+ld_status ld_local_search(const int64_t *mtx_as_vec, int32_t rows, int32_t cols, int32_t d,
+                          int32_t marginal, const int32_t *starts, int32_t n, int32_t max_rounds,
+                          int32_t device, int64_t *values, int32_t *labels);
+
 /* Labels of rows 0..rows-2 for a Gray index (the BRGC word of L_CUDA.cu:61-63,
  * the d-ary reflected word of L_CUDA.cu:204-206). */
 ld_status ld_gray_labels(uint64_t index, int32_t rows, int32_t d, int32_t *labels);

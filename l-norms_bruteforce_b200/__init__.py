@@ -54,6 +54,13 @@ class ProblemInfo(C.Structure):
                 ("max_rows", C.c_int32), ("labelings", C.c_uint64)]
 
 
+class PruneStats(C.Structure):
+    _fields_ = [("walks_total", C.c_uint64), ("walks_kept", C.c_uint64), ("highs_total", C.c_uint64),
+                ("highs_visited", C.c_uint64), ("highs_kept", C.c_uint64), ("block", C.c_uint64),
+                ("incumbent", C.c_int64), ("bound_ms", C.c_float), ("scan_ms", C.c_float),
+                ("pruned", C.c_int32), ("low_rows", C.c_int32), ("walk_rows", C.c_int32)]
+
+
 # Every exported symbol of include/lnorms_b200.h: (name, restype, argtypes)
 _P = C.c_void_p
 _I64P = C.POINTER(C.c_int64)
@@ -73,6 +80,10 @@ SIGNATURES = [
                                    C.POINTER(Result), _I32P]),
     ("ld_solve_reduced_noalloc", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            C.c_void_p, C.POINTER(Result), _I32P]),
+    ("ld_solve_pruned", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options),
+                                  _I32P, C.POINTER(Result), _I32P, C.POINTER(PruneStats)]),
+    ("ld_local_search", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _I32P, C.c_int32,
+                                  C.c_int32, C.c_int32, _I64P, _I32P]),
     ("ld_gray_labels", C.c_int, [C.c_uint64, C.c_int32, C.c_int32, _I32P]),
     ("ld_problem_report", C.c_int, [_P, C.POINTER(Result), _I32P, C.c_int32, _I32P, C.c_char_p, C.c_size_t]),
     ("ld_plan_create", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options), C.POINTER(_P)]),
@@ -171,6 +182,43 @@ def solve_reduced_noalloc(a, d: int, marginal: bool = False, device: int = 0, st
                                           C.c_void_p(stream or None), C.byref(res),
                                           labels.ctypes.data_as(_I32P)))
     return _solution(res, labels[: max(r - 1, 0)])
+
+
+def local_search(a, d: int, marginal: bool = False, starts=None, n_random: int = 64, seed: int = 0,
+                 max_rounds: int = 0, device: int = 0):
+    """Steepest-ascent single-row moves from each start (random starts when
+    `starts` is None).  Returns (values[n], labels[n, R-1])."""
+    a = _as_i64(a)
+    r, c = a.shape
+    labs_per = 2 if d == 1 else d
+    if starts is None:
+        starts = np.random.default_rng(seed).integers(0, labs_per, size=(n_random, r - 1))
+    starts = np.ascontiguousarray(np.asarray(starts, dtype=np.int32).reshape(-1, r - 1))
+    n = starts.shape[0]
+    values = np.zeros(n, dtype=np.int64)
+    labels = np.zeros((n, r - 1), dtype=np.int32)
+    _check(lib().ld_local_search(a.ctypes.data_as(_I64P), r, c, d, int(marginal),
+                                 starts.ctypes.data_as(_I32P), n, max_rounds, device,
+                                 values.ctypes.data_as(_I64P), labels.ctypes.data_as(_I32P)))
+    return values, labels
+
+
+def solve_pruned(a, d: int, marginal: bool = False, incumbent=None, opts: Options | None = None):
+    """Exact solve that skips labeling blocks whose integer upper bound is
+    below the incumbent's value (a labeling of rows 0..R-2).  Returns
+    (Solution, stats dict); the Solution equals solve_reduced's."""
+    a = _as_i64(a)
+    r, c = a.shape
+    labels = np.zeros(max(r - 1, 1), dtype=np.int32)
+    inc = None
+    if incumbent is not None:
+        inc = np.ascontiguousarray(np.asarray(incumbent, dtype=np.int32).reshape(-1))
+    res, st = Result(), PruneStats()
+    _check(lib().ld_solve_pruned(a.ctypes.data_as(_I64P), r, c, d, int(marginal),
+                                 C.byref(opts) if opts is not None else None,
+                                 inc.ctypes.data_as(_I32P) if inc is not None else None, C.byref(res),
+                                 labels.ctypes.data_as(_I32P), C.byref(st)))
+    return _solution(res, labels[: max(r - 1, 0)]), {f: getattr(st, f) for f, _ in PruneStats._fields_}
 
 
 def gray_labels(index: int, rows: int, d: int) -> np.ndarray:

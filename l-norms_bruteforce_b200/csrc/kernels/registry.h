@@ -20,6 +20,15 @@ void table_register_d3(TableKernelTab& t);
 const void* table_kernel_mixed_ptr(int D, int WB, int WA);
 // all columns in one lane width: PK = 1 (int32, W words) or 4 (int8x4, W words)
 const void* table_kernel_ptr(int D, int W, int PK);
+// pruned-search kernels {walk_bound_kernel, prune_scan_kernel} for (D, WB, WA):
+//   D = 1: WB <= 2 with WA <= 16, WB in 4, 8, .., 64 with WA = 0
+//   D = 2: WB in 4, 8, .., 48 (WA = 0) or WA in 4, 8, .., 32 (WB = 0)
+//   D = 3: WB in 4, 8, .., 32 (WA = 0) or WA in 4, 8, .., 32 (WB = 0)
+using PruneKernelTab = const void* [4][65][33][2];
+void prune_register_d1(PruneKernelTab& t);
+void prune_register_d23(PruneKernelTab& t);
+// {nullptr, nullptr} when not instantiated
+void prune_kernel_ptrs(int D, int WB, int WA, const void** bound, const void** scan);
 // wide_kernel<IT, PC, MULTI>, PC in {1,2,4,...,128}
 const void* wide_kernel_ptr(int i64, int PC, int multi);
 

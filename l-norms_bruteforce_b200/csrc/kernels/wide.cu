@@ -30,6 +30,24 @@ const void* table_kernel_ptr(int D, int W, int PK) {
   return nullptr;
 }
 
+static const PruneKernelTab& prune_kernels() {
+  static PruneKernelTab tab = {};
+  static bool init = [] {
+    prune_register_d1(tab);
+    prune_register_d23(tab);
+    return true;
+  }();
+  (void)init;
+  return tab;
+}
+
+void prune_kernel_ptrs(int D, int WB, int WA, const void** bound, const void** scan) {
+  *bound = *scan = nullptr;
+  if (D < 1 || D > 3 || WB < 0 || WB > 64 || WA < 0 || WA > 32) return;
+  *bound = prune_kernels()[D][WB][WA][0];
+  *scan = prune_kernels()[D][WB][WA][1];
+}
+
 template <typename IT, bool MULTI>
 static const void* wide_pick(int PC) {
   switch (PC) {

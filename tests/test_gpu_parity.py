@@ -207,3 +207,46 @@ def test_config2_uses_mixed_lanes(ld, workloads):
     assert f"LM is: {sol.value}" in golden["stdout"]
     assert (sol.value, sol.gray_index) == (398, 3585128208)
     plan.close()
+
+
+def prune_cases():
+    rng = np.random.default_rng(77)
+    for t in range(18):
+        d = [1, 1, 2, 3][t % 4]
+        marg = d == 1 and t % 3 == 0
+        r = {1: int(rng.integers(12, 24)), 2: int(rng.integers(12, 20)), 3: int(rng.integers(8, 13))}[d]
+        c = int(rng.integers(2, 30))
+        if t % 2:
+            u, v = rng.standard_normal((r, 2)), rng.standard_normal((2, c))
+            a = np.rint(4 * u @ v).astype(np.int64) + rng.integers(-1, 2, size=(r, c))
+        else:
+            a = rng.integers(-6, 7, size=(r, c)).astype(np.int64)
+        yield t, a, d, marg
+
+
+@pytest.mark.parametrize("case", list(prune_cases()), ids=lambda c: f"p{c[0]}")
+def test_pruned_equals_plain(ld, case):
+    _, a, d, marg = case
+    ref = O.enumerate_max(a, d, marg)
+    vals, labs = ld.local_search(a, d, marg, n_random=32, seed=1)
+    for lab in labs[:3]:
+        assert O.value(a, d, marg, lab) in vals
+    best = labs[int(np.argmax(vals))]
+    opt = O.labels(ref[1], a.shape[0], d)
+    for inc in (None, best, opt, labs[int(np.argmin(vals))]):
+        sol, st = ld.solve_pruned(a, d, marg, inc)
+        assert (sol.value, sol.gray_index) == ref, st
+        if inc is not None:
+            assert st["incumbent"] == O.value(a, d, marg, inc)
+
+
+def test_pruned_skips_most_blocks_on_low_rank(ld, workloads):
+    """With the optimum as incumbent on a low-rank 36x44 matrix, the bounds
+    prune most walks and most high indices, and the answer is unchanged."""
+    a = workloads.lowrank(36, 44, np.random.default_rng(77))
+    plain = ld.solve_reduced(a, 1)
+    sol, st = ld.solve_pruned(a, 1, False, O.labels(plain.gray_index, 36, 1))
+    assert (sol.value, sol.gray_index) == (plain.value, plain.gray_index)
+    assert st["pruned"] == 1
+    assert st["walks_kept"] < st["walks_total"] // 4
+    assert st["highs_kept"] < st["highs_total"] // 100
