@@ -230,6 +230,30 @@ void *ld_plan_result_device(const ld_plan *plan);
 void ld_plan_destroy(ld_plan *plan);
 
 /* ---------------------------------------------------------------------- */
+/* Batched solves (no counterpart in the reference: it runs one matrix per   */
+/* process).  `count` reduced matrices (mtx_as_vec layout, mats[p] with      */
+/* rows[p] x cols[p] entries, order ds[p], marginal flags margs[p] or NULL)  */
+/* are solved together: per lane class one persistent kernel pulls          */
+/* (matrix, walk range) chunks from a device work queue; the class kernels   */
+/* run concurrently and, with the per-matrix fold and the result copy, are   */
+/* captured in one CUDA graph at creation.  Matrices outside the classes     */
+/* (d >= 4, wider, 64-bit sums) get their own plans inside the same graph.   */
+/* autotune != 0 times chunk size and grid size per class on the class's     */
+/* largest matrices (cached per class shape for the process).  Results are   */
+/* the ones ld_solve_reduced gives for each matrix.                          */
+typedef struct ld_batch ld_batch;
+ld_status ld_batch_create(int32_t count, const int64_t *const *mats, const int32_t *rows,
+                          const int32_t *cols, const int32_t *ds, const int32_t *margs,
+                          const ld_options *opt, int32_t autotune, ld_batch **out);
+/* Replay the graph on the batch's stream (no host synchronisation). */
+ld_status ld_batch_launch(ld_batch *b);
+/* Wait for the last launch; values[count], gray_indices[count] (may be NULL),
+ * *ms = device time of the launch (may be NULL). */
+ld_status ld_batch_results(ld_batch *b, int64_t *values, uint64_t *gray_indices, float *ms);
+ld_status ld_batch_describe(const ld_batch *b, char *buf, size_t cap);
+void ld_batch_destroy(ld_batch *b);
+
+/* ---------------------------------------------------------------------- */
 /* The drop-in executable: `blocks threads matrix d [y|c|r] [m]`, same      */
 /* argument checks, stdout lines and strategy file as L_CUDA's main and     */
 /* arguments_CUDA (L_CUDA.cu:361-439).  Returns the process exit status.    */

@@ -84,6 +84,12 @@ SIGNATURES = [
                                   _I32P, C.POINTER(Result), _I32P, C.POINTER(PruneStats)]),
     ("ld_local_search", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _I32P, C.c_int32,
                                   C.c_int32, C.c_int32, _I64P, _I32P]),
+    ("ld_batch_create", C.c_int, [C.c_int32, C.POINTER(_I64P), _I32P, _I32P, _I32P, _I32P, C.POINTER(Options),
+                                  C.c_int32, C.POINTER(_P)]),
+    ("ld_batch_launch", C.c_int, [_P]),
+    ("ld_batch_results", C.c_int, [_P, _I64P, C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
+    ("ld_batch_describe", C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    ("ld_batch_destroy", None, [_P]),
     ("ld_gray_labels", C.c_int, [C.c_uint64, C.c_int32, C.c_int32, _I32P]),
     ("ld_problem_report", C.c_int, [_P, C.POINTER(Result), _I32P, C.c_int32, _I32P, C.c_char_p, C.c_size_t]),
     ("ld_plan_create", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Options), C.POINTER(_P)]),
@@ -395,4 +401,56 @@ class Plan:
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.ld_plan_destroy(self._h)
+            self._h = None
+
+
+class Batch:
+    """Many reduced matrices solved together: per lane class a persistent
+    kernel over a device work queue, all captured in one CUDA graph."""
+
+    def __init__(self, mats, ds, margs=None, opts: Options | None = None, autotune: bool = True):
+        self._mats = [_as_i64(m) for m in mats]
+        n = len(self._mats)
+        self.n = n
+        ptrs = (_I64P * n)(*[m.ctypes.data_as(_I64P) for m in self._mats])
+        rows = np.array([m.shape[0] for m in self._mats], dtype=np.int32)
+        cols = np.array([m.shape[1] for m in self._mats], dtype=np.int32)
+        dd = np.ascontiguousarray(np.asarray(ds, dtype=np.int32).reshape(n))
+        mm = np.ascontiguousarray(np.zeros(n, dtype=np.int32) if margs is None
+                                  else np.asarray(margs, dtype=np.int32).reshape(n))
+        h = C.c_void_p()
+        _check(lib().ld_batch_create(n, ptrs, rows.ctypes.data_as(_I32P), cols.ctypes.data_as(_I32P),
+                                     dd.ctypes.data_as(_I32P), mm.ctypes.data_as(_I32P),
+                                     C.byref(opts) if opts is not None else None, int(autotune), C.byref(h)))
+        self._h = h
+
+    def launch(self) -> None:
+        _check(lib().ld_batch_launch(self._h))
+
+    def results(self):
+        """(values int64[n], gray indices uint64[n], device ms of the launch)."""
+        v = np.zeros(self.n, dtype=np.int64)
+        g = np.zeros(self.n, dtype=np.uint64)
+        ms = C.c_float()
+        _check(lib().ld_batch_results(self._h, v.ctypes.data_as(_I64P), g.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                      C.byref(ms)))
+        return v, g, float(ms.value)
+
+    def solve(self):
+        self.launch()
+        return self.results()
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(4096)
+        _check(lib().ld_batch_describe(self._h, buf, len(buf)))
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ld_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ld_batch_destroy(self._h)
             self._h = None

@@ -29,6 +29,10 @@ void prune_register_d1(PruneKernelTab& t);
 void prune_register_d23(PruneKernelTab& t);
 // {nullptr, nullptr} when not instantiated
 void prune_kernel_ptrs(int D, int WB, int WA, const void** bound, const void** scan);
+// batch_table_kernel<D, WB, WA> for the batch lane classes (batch_inst.cu), and
+// the per-matrix fold kernel
+const void* batch_kernel_ptr(int D, int WB, int WA);
+const void* batch_fold_kernel_ptr();
 // wide_kernel<IT, PC, MULTI>, PC in {1,2,4,...,128}
 const void* wide_kernel_ptr(int i64, int PC, int multi);
 

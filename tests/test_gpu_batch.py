@@ -1,0 +1,78 @@
+"""The batched path (persistent kernel per lane class over a device work
+queue, captured in a CUDA graph) gives every matrix the value and Gray
+index the single-matrix solver gives."""
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_batch(seed, n=48):
+    rng = np.random.default_rng(seed)
+    mats, ds, ms = [], [], []
+    for t in range(n):
+        kind = t % 8
+        if kind == 0:      # int8-sized d=1
+            a = rng.integers(-3, 4, size=(int(rng.integers(6, 20)), int(rng.integers(2, 40))))
+            d, m = 1, 0
+        elif kind == 1:    # LM
+            a = rng.integers(-20, 21, size=(int(rng.integers(6, 18)), int(rng.integers(2, 30))))
+            d, m = 1, 1
+        elif kind == 2:    # d = 2
+            a = rng.integers(-30, 31, size=(int(rng.integers(6, 18)), int(rng.integers(2, 48))))
+            d, m = 2, 0
+        elif kind == 3:    # d = 3, small entries
+            a = rng.integers(-2, 3, size=(int(rng.integers(4, 11)), int(rng.integers(2, 32))))
+            d, m = 3, 0
+        elif kind == 4:    # d = 4: own plan (wide kernel)
+            a = rng.integers(-9, 10, size=(int(rng.integers(3, 8)), int(rng.integers(2, 20))))
+            d, m = 4, 0
+        elif kind == 5:    # wider than the classes: own plan
+            a = rng.integers(-9, 10, size=(int(rng.integers(4, 10)), int(rng.integers(65, 90))))
+            d, m = 1, 0
+        elif kind == 6:    # 64-bit sums: own plan
+            a = rng.integers(-2**40, 2**40, size=(int(rng.integers(3, 10)), int(rng.integers(2, 9))))
+            d, m = 1, 0
+        else:              # single row
+            a = rng.integers(-9, 10, size=(1, int(rng.integers(1, 9))))
+            d, m = int(rng.choice([1, 2, 3])), 0
+        mats.append(np.asarray(a, dtype=np.int64)); ds.append(d); ms.append(m)
+    return mats, ds, ms
+
+
+@pytest.mark.parametrize("autotune", [False, True])
+def test_batch_matches_single_solves(ld, autotune):
+    mats, ds, ms = mixed_batch(3)
+    b = ld.Batch(mats, ds, ms, autotune=autotune)
+    v, g, t = b.solve()
+    for p, (a, d, m) in enumerate(zip(mats, ds, ms)):
+        ref = O.enumerate_max(a, d, bool(m))
+        assert (int(v[p]), int(g[p])) == ref, (p, a.shape, d, m, b.describe())
+    # the captured graph replays to the same results
+    v2, g2, t2 = b.solve()
+    assert np.array_equal(v, v2) and np.array_equal(g, g2)
+    assert t > 0 and t2 > 0
+    b.close()
+
+
+def test_batch_of_config4_sample(ld, workloads):
+    """A slice of the 4096-matrix configuration (entries N(0, 20^2), d in
+    {1,2,3}); matrices with more than 2^22 labelings are left out so the
+    oracle check stays fast."""
+    insts = [i for i in workloads.config4(count=400, seed=4)]
+    mats, ds = [], []
+    for inst in insts:
+        p = ld.Problem.from_matrix(inst.matrix, inst.d)
+        info = p.info
+        if info["labelings"] > (1 << 22):
+            continue
+        mats.append(p.reduced); ds.append(info["d"])
+    assert len(mats) > 50
+    b = ld.Batch(mats, ds, autotune=True)
+    v, g, _ = b.solve()
+    for p, (a, d) in enumerate(zip(mats, ds)):
+        sol = ld.solve_reduced(a, d)
+        assert (int(v[p]), int(g[p])) == (sol.value, sol.gray_index), p
+    b.close()
