@@ -999,7 +999,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         if (c.WB == 0) { c.WA = round4(c.WA); }
         else {
           c.WB = (C + 7) & ~7; c.WA = 0;
-          if (c.WB > (d == 1 ? 64 : d == 2 ? 48 : 32)) continue;
+          if (c.WB > (d == 1 ? 64 : d == 2 ? 64 : 48)) continue;
           // with all-int32 lanes the column order is the identity and every column is wide
         }
         c.WT = round4(c.WB + c.WA);
@@ -1176,10 +1176,10 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     int best_wpt = 1;
     double best_frac = 1.0;
     for (int wpt : {1, 2, 4, 8}) {
-      for (double frac : {1.0, 0.5}) {
+      for (double frac : {1.0}) {
         std::vector<ld::BatchChunk> chunks;
         batch_chunks(b, c, wpt, walks, &chunks);
-        const int sample = std::min<int>((int)chunks.size(), 4 * di.sms * c.bps);
+        const int sample = std::min<int>((int)chunks.size(), 2 * di.sms * c.bps);
         if (sample < 1) continue;
         cudaMemcpy(b->dmem + b->off_chunks, chunks.data(), sizeof(ld::BatchChunk) * sample, cudaMemcpyHostToDevice);
         BatchClass tc = c;
@@ -1189,7 +1189,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         args.nchunks = sample;
         args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres);
         float ms = 0;
-        for (int rep = 0; rep < 2; ++rep) {
+        for (int rep = 0; rep < 1; ++rep) {
           cudaMemsetAsync(args.head, 0, sizeof(unsigned int), b->stream);
           cudaEventRecord(b->ev0, b->stream);
           void* params[] = {&args};
@@ -1219,7 +1219,6 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   cudaStream_t s = b->stream;
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->dmem + b->off_heads, 0, sizeof(unsigned int) * std::max<size_t>(1, b->classes.size()), s);
-  if (e == cudaSuccess) e = cudaEventRecord(b->ev0, s);
   if (e == cudaSuccess) e = cudaEventRecord(b->fork, s);
   for (auto& c : b->classes) {
     if (e != cudaSuccess) break;
@@ -1246,7 +1245,6 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     if (b->plans[p])
       e = cudaMemcpyAsync(b->dmem + b->off_res + sizeof(ld::Slot) * p, b->plans[p]->red.result, sizeof(ld::Slot),
                           cudaMemcpyDeviceToDevice, s);
-  if (e == cudaSuccess) e = cudaEventRecord(b->ev1, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->hres, b->dmem + b->off_res, sizeof(ld::Slot) * count, cudaMemcpyDeviceToHost, s);
   cudaGraph_t g = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(s, &g);
@@ -1273,7 +1271,10 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
 extern "C" ld_status ld_batch_launch(ld_batch* b) {
   if (!b || !b->exec) return ld_fail(LD_ERR_ARG, "null batch");
   LD_CUDA(cudaSetDevice(b->device));
+  // timing events outside the graph (events recorded during capture cannot be timed)
+  LD_CUDA(cudaEventRecord(b->ev0, b->stream));
   LD_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  LD_CUDA(cudaEventRecord(b->ev1, b->stream));
   b->launched = true;
   return LD_OK;
 }
