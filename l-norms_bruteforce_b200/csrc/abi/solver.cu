@@ -999,7 +999,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         if (c.WB == 0) { c.WA = round4(c.WA); }
         else {
           c.WB = (C + 7) & ~7; c.WA = 0;
-          if (c.WB > (d == 1 ? 64 : d == 2 ? 64 : 48)) continue;
+          if (c.WB > 64) continue;
           // with all-int32 lanes the column order is the identity and every column is wide
         }
         c.WT = round4(c.WB + c.WA);

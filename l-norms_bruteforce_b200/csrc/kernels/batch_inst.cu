@@ -1,7 +1,7 @@
 // Batched persistent kernel instances (lane classes) and their lookup:
 //   D = 1: int32 words 8, 16, .., 64 or int8x4 words 4, 8, .., 32
 //   D = 2: int32 words 8, 16, .., 64 or int8x4 words 4, 8, .., 32
-//   D = 3: int32 words 8, 16, .., 48 or int8x4 words 4, 8, .., 32
+//   D = 3: int32 words 8, 16, .., 64 or int8x4 words 4, 8, .., 32
 #include <utility>
 
 #include "batch_kernel.cuh"
@@ -26,7 +26,7 @@ const BatchTab& batch_kernels() {
   static bool init = [] {
     fill_b32<1>(tab, std::make_integer_sequence<int, 8>{});
     fill_b32<2>(tab, std::make_integer_sequence<int, 8>{});
-    fill_b32<3>(tab, std::make_integer_sequence<int, 6>{});
+    fill_b32<3>(tab, std::make_integer_sequence<int, 8>{});
     fill_b8<1>(tab, std::make_integer_sequence<int, 8>{});
     fill_b8<2>(tab, std::make_integer_sequence<int, 8>{});
     fill_b8<3>(tab, std::make_integer_sequence<int, 8>{});

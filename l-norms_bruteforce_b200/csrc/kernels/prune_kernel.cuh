@@ -50,6 +50,7 @@ constexpr int kPruneThreads = 128;
 template <int D, int WB, int WA>
 __device__ __forceinline__ long long prefix_abs(const uint32_t* H, const uint32_t* T) {
   using S = Shape<D, WB, WA>;
+  static_assert(D != 3 || S::NR == 3, "pruned d = 3 shapes keep H1 + H2 in registers");
   uint32_t acc = 0u;
   if (D == 1) {
 #pragma unroll
@@ -98,8 +99,8 @@ __device__ __forceinline__ void seed_top(uint32_t* H, const uint32_t* sA, const 
       const int lab = r < 3 ? r : 5 - r;
       q /= 3ull;
       const uint32_t* row = sA + (k + t) * S::WT;
-      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); add_row<D, WB, WA>(H, row, 2); }
-      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); add_row<D, WB, WA>(H, row, 2); }
+      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); if (S::NR == 3) add_row<D, WB, WA>(H, row, 2); }
+      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); if (S::NR == 3) add_row<D, WB, WA>(H, row, 2); }
     }
   }
 }
@@ -124,8 +125,8 @@ __device__ __forceinline__ void add_walk_rows(uint32_t* H, const uint32_t* sA, i
       const int lab = r < 3 ? r : 5 - r;
       q /= 3ull;
       const uint32_t* row = sA + (k + t) * S::WT;
-      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); add_row<D, WB, WA>(H, row, 2); }
-      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); add_row<D, WB, WA>(H, row, 2); }
+      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); if (S::NR == 3) add_row<D, WB, WA>(H, row, 2); }
+      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); if (S::NR == 3) add_row<D, WB, WA>(H, row, 2); }
     }
   }
 }

@@ -7,7 +7,7 @@ namespace ld {
 // WA int8x4 words (0..32).  Instances:
 //   D = 1: WB <= 4 with WA <= 16 (mixed), WA <= 32 with WB = 0, WB <= 64 with WA = 0
 //   D = 2: WB <= 64 with WA = 0, WA <= 32 with WB = 0
-//   D = 3: WB <= 48 with WA = 0, WA <= 32 with WB = 0
+//   D = 3: WB <= 64 with WA = 0, WA <= 32 with WB = 0
 using TableKernelTab = const void* [4][65][33];
 void table_register_d1_mix(TableKernelTab& t);
 void table_register_d1_p8(TableKernelTab& t);

@@ -31,7 +31,8 @@
 //     both table vectors are compared against the same register vector H
 //     (|H + L1| + |H - (T - L1)|);
 //   D = 3 (L_3):      s1, s2, s0 = T - s1 - s2;            table: -L1, -L2, T-L1-L2
-//     with registers H1, H2 and H1+H2.
+//     with registers H1, H2 and H1+H2 (above 32 words per vector H1+H2 is
+//     formed on the fly from H1 and H2 to stay within the register file).
 // LM enters as L_1 with column 0 shifted by K = sum_i |A_i0|: K_H (the
 // high and fixed rows' share) is added to H's column 0 and K_L (the low
 // rows' share) is subtracted through the table bias tb, so that column's
@@ -74,7 +75,8 @@ struct Shape {
   static constexpr int WV = WB + WA;                  // computed words per vector
   static constexpr int WT = (WV + 3) & ~3;            // padded words per vector
   static constexpr int NW = D * WT;                   // words per table entry
-  static constexpr int NR = D == 3 ? 3 : 1;           // register vectors
+  // register vectors: D = 3 keeps H1, H2 and (up to 32 words) H1 + H2
+  static constexpr int NR = D == 3 ? (WV > 32 ? 2 : 3) : 1;
 };
 
 template <int WB>
@@ -117,8 +119,10 @@ __device__ __forceinline__ void move_row(uint32_t* H, const uint32_t* row, int a
     if (a == 2) sub_row<D, WB, WA>(H, row, 1);
     if (b == 1) add_row<D, WB, WA>(H, row, 0);
     if (b == 2) add_row<D, WB, WA>(H, row, 1);
-    if (a == 0 && b != 0) add_row<D, WB, WA>(H, row, 2);
-    if (a != 0 && b == 0) sub_row<D, WB, WA>(H, row, 2);
+    if (Shape<D, WB, WA>::NR == 3) {
+      if (a == 0 && b != 0) add_row<D, WB, WA>(H, row, 2);
+      if (a != 0 && b == 0) sub_row<D, WB, WA>(H, row, 2);
+    }
   }
 }
 
@@ -148,8 +152,8 @@ __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const
       const int lab = r < 3 ? r : 5 - r;
       q /= 3ull;
       const uint32_t* row = sA + (k + t) * S::WT;
-      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); add_row<D, WB, WA>(H, row, 2); }
-      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); add_row<D, WB, WA>(H, row, 2); }
+      if (lab == 1) { add_row<D, WB, WA>(H, row, 0); if (S::NR == 3) add_row<D, WB, WA>(H, row, 2); }
+      else if (lab == 2) { add_row<D, WB, WA>(H, row, 1); if (S::NR == 3) add_row<D, WB, WA>(H, row, 2); }
     }
   }
 }
@@ -176,7 +180,11 @@ __device__ __forceinline__ void sad4(const uint32_t* H, const uint4& x, int q, u
     const int tq = 4 * q + c;
     if (computed<D, WB, WA>(tq)) {
       uint32_t& acc = (c & 1) ? a1 : a0;
-      acc = wsad<WB>(tq % S::WT, H[reg_of<D, WB, WA>(tq)], xs[c], acc);
+      const int w = tq % S::WT;
+      if (D == 3 && S::NR == 2 && tq / S::WT == 2)   // H1 + H2, formed on the fly
+        acc = wsad<WB>(w, wadd<WB>(w, H[w], H[S::WV + w]), xs[c], acc);
+      else
+        acc = wsad<WB>(w, H[reg_of<D, WB, WA>(tq)], xs[c], acc);
     }
   }
 }

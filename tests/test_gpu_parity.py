@@ -250,3 +250,16 @@ def test_pruned_skips_most_blocks_on_low_rank(ld, workloads):
     assert st["pruned"] == 1
     assert st["walks_kept"] < st["walks_total"] // 4
     assert st["highs_kept"] < st["highs_total"] // 100
+
+
+@pytest.mark.parametrize("cols", [33, 41, 48, 57, 64])
+def test_d3_above_32_words(ld, cols):
+    """d = 3 with more than 32 column words keeps H1, H2 and forms H1+H2 on
+    the fly; d = 2 up to 64 words."""
+    rng = np.random.default_rng(cols)
+    a = rng.integers(-60, 61, size=(9, cols)).astype(np.int64)
+    for d in (2, 3):
+        plan = ld.Plan(a, d, False, ld.options(kernel=1, lane_bits=32))
+        sol = plan.solve()
+        assert (sol.value, sol.gray_index) == O.enumerate_max(a, d, False), plan.describe()
+        plan.close()
