@@ -240,6 +240,7 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     ld = load_package()
+    import lnorms_b200.distributed as D
     inst = instance(args.config)
     prob = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
     info = prob.info
@@ -311,9 +312,8 @@ def run_ours(args) -> None:
         p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
         res = p.solve(ld.options(device=local, shard_index=rank, shard_count=world))
         if world > 1:
-            pair = torch.tensor([res.value, res.gray_index], dtype=torch.int64, device="cuda")
-            v, idx = combine(pair)
-            res.value, res.gray_index = int(v.item()), int(idx.item())
+            res.value, res.gray_index = D.combine(int(res.value), int(res.gray_index),
+                                                  device=torch.device("cuda", local))
         p.report(res)
         dt = (time.perf_counter() - t0) * 1e3
         if i >= args.warmup:
