@@ -254,6 +254,36 @@ ld_status ld_batch_describe(const ld_batch *b, char *buf, size_t cap);
 void ld_batch_destroy(ld_batch *b);
 
 /* ---------------------------------------------------------------------- */
+/* Proposal network for the pruned search (no counterpart in the reference): */
+/* a 44 -> 256 -> 256 -> 44 ReLU perceptron whose GEMMs run on the tensor    */
+/* cores (bf16 operands, fp32 accumulation, tcgen05 + TMEM), trained with    */
+/* Adam on fp32 master weights against masked binary cross-entropy.  Rows   */
+/* of x are 44 features, rows of t / mask 44 targets in [0,1] and weights   */
+/* (0 drops an entry).  Parameters travel as one flat fp32 array: W1[256x44] */
+/* b1[256] W2[256x256] b2[256] W3[44x256] b3[44] (ld_mlp_param_count()).    */
+typedef struct ld_mlp ld_mlp;
+/* batch: rows per device pass, a positive multiple of 128. */
+ld_status ld_mlp_create(int32_t batch, uint64_t seed, int32_t device, ld_mlp **out);
+int64_t ld_mlp_param_count(void);
+ld_status ld_mlp_get_params(ld_mlp *net, float *params);
+ld_status ld_mlp_set_params(ld_mlp *net, const float *params);
+/* logits[rows x 44] for x[rows x 44]; any number of rows. */
+ld_status ld_mlp_forward(ld_mlp *net, const float *x, int32_t rows, float *logits);
+/* Gradients of the mean masked loss (flat parameter layout; grads or loss
+ * may be NULL) for rows <= batch, no update. */
+ld_status ld_mlp_gradients(ld_mlp *net, const float *x, const float *t, const float *mask,
+                           int32_t rows, float *grads, float *loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on rows <= batch. */
+ld_status ld_mlp_train_step(ld_mlp *net, const float *x, const float *t, const float *mask,
+                            int32_t rows, float lr, float *loss);
+void ld_mlp_destroy(ld_mlp *net);
+/* The tensor-core GEMM alone, for tests: C[M x N] (fp32) = A[M x K] *      */
+/* B[N x K]^T with A, B given as bf16 bit patterns; M % 128 == 0,           */
+/* N % 64 == 0, K % 64 == 0. */
+ld_status ld_tc_gemm(const uint16_t *A, const uint16_t *B, int32_t M, int32_t N, int32_t K,
+                     float *C, int32_t device);
+
+/* ---------------------------------------------------------------------- */
 /* The drop-in executable: `blocks threads matrix d [y|c|r] [m]`, same      */
 /* argument checks, stdout lines and strategy file as L_CUDA's main and     */
 /* arguments_CUDA (L_CUDA.cu:361-439).  Returns the process exit status.    */

@@ -65,6 +65,7 @@ class PruneStats(C.Structure):
 _P = C.c_void_p
 _I64P = C.POINTER(C.c_int64)
 _I32P = C.POINTER(C.c_int32)
+_F32P = C.POINTER(C.c_float)
 SIGNATURES = [
     ("ld_options_init", None, [C.POINTER(Options)]),
     ("ld_problem_from_text", C.c_int, [C.c_char_p, C.c_size_t, C.c_int32, C.c_char, C.c_int32, C.POINTER(_P)]),
@@ -100,6 +101,16 @@ SIGNATURES = [
     ("ld_plan_stream", C.c_void_p, [_P]),
     ("ld_plan_result_device", C.c_void_p, [_P]),
     ("ld_plan_destroy", None, [_P]),
+    ("ld_mlp_create", C.c_int, [C.c_int32, C.c_uint64, C.c_int32, C.POINTER(_P)]),
+    ("ld_mlp_param_count", C.c_int64, []),
+    ("ld_mlp_get_params", C.c_int, [_P, _F32P]),
+    ("ld_mlp_set_params", C.c_int, [_P, _F32P]),
+    ("ld_mlp_forward", C.c_int, [_P, _F32P, C.c_int32, _F32P]),
+    ("ld_mlp_gradients", C.c_int, [_P, _F32P, _F32P, _F32P, C.c_int32, _F32P, _F32P]),
+    ("ld_mlp_train_step", C.c_int, [_P, _F32P, _F32P, _F32P, C.c_int32, C.c_float, _F32P]),
+    ("ld_mlp_destroy", None, [_P]),
+    ("ld_tc_gemm", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_int32, C.c_int32, C.c_int32,
+                             _F32P, C.c_int32]),
     ("ld_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("ld_measure_int32_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("ld_last_error", C.c_char_p, []),
@@ -454,3 +465,104 @@ class Batch:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.ld_batch_destroy(self._h)
             self._h = None
+
+
+# ---------------------------------------------------------------------------
+# proposal network (tensor-core MLP 44 -> 256 -> 256 -> 44)
+
+MLP_IN = 44
+MLP_HIDDEN = 256
+MLP_OUT = 44
+MLP_SHAPES = [("W1", (MLP_HIDDEN, MLP_IN)), ("b1", (MLP_HIDDEN,)), ("W2", (MLP_HIDDEN, MLP_HIDDEN)),
+              ("b2", (MLP_HIDDEN,)), ("W3", (MLP_OUT, MLP_HIDDEN)), ("b3", (MLP_OUT,))]
+
+
+def _f32(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def unflatten_params(flat: np.ndarray) -> dict:
+    out, off = {}, 0
+    for name, shape in MLP_SHAPES:
+        n = int(np.prod(shape))
+        out[name] = flat[off:off + n].reshape(shape)
+        off += n
+    return out
+
+
+def flatten_params(p: dict) -> np.ndarray:
+    return np.concatenate([np.asarray(p[name], dtype=np.float32).reshape(-1) for name, _ in MLP_SHAPES])
+
+
+class Mlp:
+    """The proposal network on one GPU: forward, gradients and Adam steps run
+    on the library's tensor-core kernels (bf16 operands, fp32 accumulate)."""
+
+    def __init__(self, batch: int = 1024, seed: int = 0, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().ld_mlp_create(int(batch), int(seed), int(device), C.byref(h)))
+        self._h = h
+        self.batch = int(batch)
+
+    @staticmethod
+    def param_count() -> int:
+        return int(lib().ld_mlp_param_count())
+
+    def get_params(self) -> dict:
+        flat = np.zeros(self.param_count(), dtype=np.float32)
+        _check(lib().ld_mlp_get_params(self._h, flat.ctypes.data_as(_F32P)))
+        return unflatten_params(flat)
+
+    def set_params(self, params: dict) -> None:
+        flat = _f32(flatten_params(params))
+        _check(lib().ld_mlp_set_params(self._h, flat.ctypes.data_as(_F32P)))
+
+    def forward(self, x) -> np.ndarray:
+        x = _f32(x)
+        rows = x.shape[0]
+        out = np.zeros((rows, MLP_OUT), dtype=np.float32)
+        _check(lib().ld_mlp_forward(self._h, x.ctypes.data_as(_F32P), rows, out.ctypes.data_as(_F32P)))
+        return out
+
+    def gradients(self, x, t, mask):
+        x, t, mask = _f32(x), _f32(t), _f32(mask)
+        flat = np.zeros(self.param_count(), dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().ld_mlp_gradients(self._h, x.ctypes.data_as(_F32P), t.ctypes.data_as(_F32P),
+                                      mask.ctypes.data_as(_F32P), x.shape[0], flat.ctypes.data_as(_F32P),
+                                      C.byref(loss)))
+        return unflatten_params(flat), float(loss.value)
+
+    def train_step(self, x, t, mask, lr: float = 1e-3) -> float:
+        x, t, mask = _f32(x), _f32(t), _f32(mask)
+        loss = C.c_float()
+        _check(lib().ld_mlp_train_step(self._h, x.ctypes.data_as(_F32P), t.ctypes.data_as(_F32P),
+                                       mask.ctypes.data_as(_F32P), x.shape[0], float(lr), C.byref(loss)))
+        return float(loss.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ld_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ld_mlp_destroy(self._h)
+            self._h = None
+
+
+def tc_gemm(a_bits: np.ndarray, b_bits: np.ndarray, device: int = 0) -> np.ndarray:
+    """C = A B^T on the tensor cores; A, B are bf16 bit patterns (uint16)."""
+    a = np.ascontiguousarray(a_bits, dtype=np.uint16)
+    b = np.ascontiguousarray(b_bits, dtype=np.uint16)
+    M, K = a.shape
+    N = b.shape[0]
+    if b.shape[1] != K:
+        raise ValueError("inner dimensions differ")
+    c = np.zeros((M, N), dtype=np.float32)
+    _check(lib().ld_tc_gemm(a.ctypes.data_as(C.POINTER(C.c_uint16)), b.ctypes.data_as(C.POINTER(C.c_uint16)),
+                            M, N, K, c.ctypes.data_as(_F32P), int(device)))
+    return c

@@ -1,0 +1,354 @@
+// The proposal network: 44 -> 256 -> 256 -> 44, ReLU, bf16 operands with
+// fp32 accumulation on the tensor cores (mlp_tc.cuh), trained with Adam on
+// fp32 master weights.  Every GEMM of the forward and backward passes is
+// C = A * B^T with both operands K-major; transposed copies of activations,
+// gradients and weights are written by the kernels that produce them.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "../host/ld_internal.h"
+#include "../kernels/mlp_tc.cuh"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int kIn = 44, kInP = 64, kHid = 256, kOut = 44, kOutP = 64, kOutGP = 128;
+
+#define MLP_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return ld_fail(LD_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+template <int BN>
+cudaError_t launch_gemm(const ld::mlp::GemmArgs& g, cudaStream_t s) {
+  // Each CTA holds BN of the SM's 512 TMEM columns; the shared-memory request
+  // is raised so that no more CTAs share an SM than TMEM can hold at once
+  // (233472 bytes of shared memory per SM, 1 KB reserved per CTA).
+  const size_t tiles = (size_t)ld::mlp::kTileM * ld::mlp::kTileK * 2 + (size_t)BN * ld::mlp::kTileK * 2;
+  const size_t cap = 233472 / (512 / BN + 1) + 1024;
+  const size_t smem = tiles > cap ? tiles : cap;
+  cudaError_t e = cudaFuncSetAttribute(ld::mlp::tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(g.M / ld::mlp::kTileM, g.N / BN);
+  ld::mlp::tc_gemm_kernel<BN><<<grid, 128, smem, s>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t gemm(const bf16* A, const bf16* B, int M, int N, int K, float* C, bf16* H, bf16* HT,
+                 const float* bias, int relu, int* err, cudaStream_t s) {
+  ld::mlp::GemmArgs g{A, B, M, N, K, C, H, HT, bias, relu, err};
+  if (N % 256 == 0) return launch_gemm<256>(g, s);
+  if (N % 128 == 0) return launch_gemm<128>(g, s);
+  return launch_gemm<64>(g, s);
+}
+
+int blocks_for(int n, int t = 256) { return (n + t - 1) / t; }
+
+}  // namespace
+
+struct ld_mlp {
+  int device = 0, batch = 0;
+  cudaStream_t s = nullptr;
+  void* mem = nullptr;
+  // fp32 master parameters (padded shapes), gradients, Adam moments
+  float *W1, *b1, *W2, *b2, *W3, *b3;
+  float *gW1, *gb1, *gW2, *gb2, *gW3, *gb3;
+  float *m[6], *v[6];
+  // bf16 operands
+  bf16 *W1b, *W2b, *W2T, *W3b, *W3T;
+  bf16 *Xb, *XT, *H1, *H1T, *H2, *H2T, *dZ3, *dZ3T, *dZ2, *dZ2T, *dZ1T;
+  float *Xf, *Z3, *Tt, *Mk, *dH2, *dH1, *loss;
+  int* err;
+  int step = 0;
+};
+
+namespace {
+
+// parameter shapes (rows, cols) in the padded device layout and in the flat
+// host layout used by get/set (unpadded)
+struct PShape { int rows, cols, hrows, hcols; };
+const PShape kShapes[6] = {{kHid, kInP, kHid, kIn}, {1, kHid, 1, kHid},   {kHid, kHid, kHid, kHid},
+                           {1, kHid, 1, kHid},      {kOutP, kHid, kOut, kHid}, {1, kOutP, 1, kOut}};
+
+float** params_of(ld_mlp* n, int i) {
+  float** arr[6] = {&n->W1, &n->b1, &n->W2, &n->b2, &n->W3, &n->b3};
+  return arr[i];
+}
+float** grads_of(ld_mlp* n, int i) {
+  float** arr[6] = {&n->gW1, &n->gb1, &n->gW2, &n->gb2, &n->gW3, &n->gb3};
+  return arr[i];
+}
+
+size_t host_param_count() {
+  size_t c = 0;
+  for (const auto& s : kShapes) c += (size_t)s.hrows * s.hcols;
+  return c;
+}
+
+// refresh the bf16 copies of the weights from the fp32 masters
+cudaError_t refresh_bf16(ld_mlp* n) {
+  ld::mlp::to_bf16_kernel<<<blocks_for(kHid * kInP), 256, 0, n->s>>>(n->W1, kHid, kInP, n->W1b, nullptr);
+  ld::mlp::to_bf16_kernel<<<blocks_for(kHid * kHid), 256, 0, n->s>>>(n->W2, kHid, kHid, n->W2b, n->W2T);
+  ld::mlp::to_bf16_kernel<<<blocks_for(kOutP * kHid), 256, 0, n->s>>>(n->W3, kOutP, kHid, n->W3b, n->W3T);
+  return cudaGetLastError();
+}
+
+ld_status upload_batch(ld_mlp* n, const float* x, const float* t, const float* mask, int rows) {
+  std::vector<float> X((size_t)n->batch * kInP, 0.f), T, M;
+  for (int r = 0; r < rows; ++r) memcpy(&X[(size_t)r * kInP], x + (size_t)r * kIn, sizeof(float) * kIn);
+  MLP_CUDA(cudaMemcpyAsync(n->Xf, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, n->s));
+  if (t) {
+    T.assign((size_t)n->batch * kOutP, 0.f);
+    M.assign((size_t)n->batch * kOutP, 0.f);
+    for (int r = 0; r < rows; ++r)
+      for (int c = 0; c < kOut; ++c) {
+        T[(size_t)r * kOutP + c] = t[(size_t)r * kOut + c];
+        M[(size_t)r * kOutP + c] = mask[(size_t)r * kOut + c];
+      }
+    MLP_CUDA(cudaMemcpyAsync(n->Tt, T.data(), sizeof(float) * T.size(), cudaMemcpyHostToDevice, n->s));
+    MLP_CUDA(cudaMemcpyAsync(n->Mk, M.data(), sizeof(float) * M.size(), cudaMemcpyHostToDevice, n->s));
+  }
+  ld::mlp::to_bf16_kernel<<<blocks_for(n->batch * kInP), 256, 0, n->s>>>(n->Xf, n->batch, kInP, n->Xb, n->XT);
+  MLP_CUDA(cudaGetLastError());
+  return LD_OK;
+}
+
+ld_status forward(ld_mlp* n) {
+  const int B = n->batch;
+  MLP_CUDA(gemm(n->Xb, n->W1b, B, kHid, kInP, nullptr, n->H1, n->H1T, n->b1, 1, n->err, n->s));
+  MLP_CUDA(gemm(n->H1, n->W2b, B, kHid, kHid, nullptr, n->H2, n->H2T, n->b2, 1, n->err, n->s));
+  MLP_CUDA(gemm(n->H2, n->W3b, B, kOutP, kHid, n->Z3, nullptr, nullptr, n->b3, 0, n->err, n->s));
+  return LD_OK;
+}
+
+ld_status backward(ld_mlp* n, float inv_count) {
+  const int B = n->batch;
+  MLP_CUDA(cudaMemsetAsync(n->loss, 0, sizeof(float), n->s));
+  ld::mlp::bce_grad_kernel<<<blocks_for(B * kOutP), 256, 0, n->s>>>(n->Z3, n->Tt, n->Mk, B, kOutP, inv_count,
+                                                                     n->dZ3, n->dZ3T, n->loss);
+  MLP_CUDA(cudaGetLastError());
+  // W3: [kOutGP x B] x [kHid x B]^T (rows kOutP.. of dZ3T are zero)
+  MLP_CUDA(gemm(n->dZ3T, n->H2T, kOutGP, kHid, B, n->gW3, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  MLP_CUDA(gemm(n->dZ3, n->W3T, B, kHid, kOutP, n->dH2, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  ld::mlp::relu_grad_kernel<<<blocks_for(B * kHid), 256, 0, n->s>>>(n->dH2, n->H2, B, kHid, n->dZ2, n->dZ2T);
+  MLP_CUDA(cudaGetLastError());
+  MLP_CUDA(gemm(n->dZ2T, n->H1T, kHid, kHid, B, n->gW2, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  MLP_CUDA(gemm(n->dZ2, n->W2T, B, kHid, kHid, n->dH1, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  ld::mlp::relu_grad_kernel<<<blocks_for(B * kHid), 256, 0, n->s>>>(n->dH1, n->H1, B, kHid, nullptr, n->dZ1T);
+  MLP_CUDA(cudaGetLastError());
+  MLP_CUDA(gemm(n->dZ1T, n->XT, kHid, kInP, B, n->gW1, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  ld::mlp::bias_grad_kernel<<<kHid / 4, 128, 0, n->s>>>(n->dZ1T, kHid, B, n->gb1);
+  ld::mlp::bias_grad_kernel<<<kHid / 4, 128, 0, n->s>>>(n->dZ2T, kHid, B, n->gb2);
+  ld::mlp::bias_grad_kernel<<<kOutP / 4, 128, 0, n->s>>>(n->dZ3T, kOutP, B, n->gb3);
+  MLP_CUDA(cudaGetLastError());
+  return LD_OK;
+}
+
+ld_status check_err(ld_mlp* n) {
+  int e = 0;
+  MLP_CUDA(cudaMemcpyAsync(&e, n->err, sizeof e, cudaMemcpyDeviceToHost, n->s));
+  MLP_CUDA(cudaStreamSynchronize(n->s));
+  if (e) {
+    cudaMemsetAsync(n->err, 0, sizeof(int), n->s);
+    return ld_fail(LD_ERR_TIMEOUT, "tensor-core GEMM wait ran out (code %d)", e);
+  }
+  return LD_OK;
+}
+
+}  // namespace
+
+extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, int32_t device, ld_mlp** out) {
+  if (!out || batch < 128 || batch % 128) return ld_fail(LD_ERR_ARG, "batch must be a positive multiple of 128");
+  if (cudaSetDevice(device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "no device %d", device);
+  ld_mlp* n = new ld_mlp();
+  n->device = device;
+  n->batch = batch;
+  const int B = batch;
+  // one allocation, carved in 256-byte aligned pieces
+  struct Piece { void** p; size_t bytes; };
+  std::vector<Piece> pieces;
+  auto f32 = [&](float** p, size_t count) { pieces.push_back({(void**)p, count * 4}); };
+  auto b16 = [&](bf16** p, size_t count) { pieces.push_back({(void**)p, count * 2}); };
+  for (int i = 0; i < 6; ++i) {
+    const size_t c = (size_t)kShapes[i].rows * kShapes[i].cols;
+    f32(params_of(n, i), c);
+    f32(grads_of(n, i), i == 4 ? (size_t)kOutGP * kHid : c);
+    f32(&n->m[i], c);
+    f32(&n->v[i], c);
+  }
+  b16(&n->W1b, (size_t)kHid * kInP); b16(&n->W2b, (size_t)kHid * kHid); b16(&n->W2T, (size_t)kHid * kHid);
+  b16(&n->W3b, (size_t)kOutP * kHid); b16(&n->W3T, (size_t)kHid * kOutP);
+  b16(&n->Xb, (size_t)B * kInP); b16(&n->XT, (size_t)kInP * B);
+  b16(&n->H1, (size_t)B * kHid); b16(&n->H1T, (size_t)kHid * B);
+  b16(&n->H2, (size_t)B * kHid); b16(&n->H2T, (size_t)kHid * B);
+  b16(&n->dZ3, (size_t)B * kOutP); b16(&n->dZ3T, (size_t)kOutGP * B);
+  b16(&n->dZ2, (size_t)B * kHid); b16(&n->dZ2T, (size_t)kHid * B); b16(&n->dZ1T, (size_t)kHid * B);
+  f32(&n->Xf, (size_t)B * kInP); f32(&n->Z3, (size_t)B * kOutP); f32(&n->Tt, (size_t)B * kOutP);
+  f32(&n->Mk, (size_t)B * kOutP); f32(&n->dH2, (size_t)B * kHid); f32(&n->dH1, (size_t)B * kHid);
+  f32(&n->loss, 1);
+  pieces.push_back({(void**)&n->err, 4});
+  size_t total = 0;
+  for (auto& pc : pieces) total += (pc.bytes + 255) & ~(size_t)255;
+  if (cudaMalloc(&n->mem, total) != cudaSuccess || cudaStreamCreateWithFlags(&n->s, cudaStreamNonBlocking) != cudaSuccess) {
+    if (n->mem) cudaFree(n->mem);
+    delete n;
+    return ld_fail(LD_ERR_CUDA, "network allocation of %zu bytes failed", total);
+  }
+  cudaMemset(n->mem, 0, total);
+  size_t off = 0;
+  for (auto& pc : pieces) { *pc.p = (char*)n->mem + off; off += (pc.bytes + 255) & ~(size_t)255; }
+  // He-uniform initialisation of the real (unpadded) weights, zero biases
+  std::mt19937_64 rng(seed);
+  for (int i = 0; i < 6; i += 2) {
+    const PShape& sh = kShapes[i];
+    std::vector<float> w((size_t)sh.rows * sh.cols, 0.f);
+    const float lim = std::sqrt(6.f / (float)sh.hcols);
+    std::uniform_real_distribution<float> U(-lim, lim);
+    for (int r = 0; r < sh.hrows; ++r)
+      for (int c = 0; c < sh.hcols; ++c) w[(size_t)r * sh.cols + c] = U(rng);
+    cudaMemcpy(*params_of(n, i), w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
+  }
+  if (refresh_bf16(n) != cudaSuccess || cudaStreamSynchronize(n->s) != cudaSuccess) {
+    ld_mlp_destroy(n);
+    return ld_fail(LD_ERR_CUDA, "network initialisation failed");
+  }
+  *out = n;
+  return LD_OK;
+}
+
+extern "C" void ld_mlp_destroy(ld_mlp* n) {
+  if (!n) return;
+  cudaSetDevice(n->device);
+  if (n->s) { cudaStreamSynchronize(n->s); cudaStreamDestroy(n->s); }
+  if (n->mem) cudaFree(n->mem);
+  delete n;
+}
+
+extern "C" int64_t ld_mlp_param_count(void) { return (int64_t)host_param_count(); }
+
+extern "C" ld_status ld_mlp_get_params(ld_mlp* n, float* params) {
+  if (!n || !params) return ld_fail(LD_ERR_ARG, "null argument");
+  MLP_CUDA(cudaSetDevice(n->device));
+  MLP_CUDA(cudaStreamSynchronize(n->s));
+  float* dst = params;
+  for (int i = 0; i < 6; ++i) {
+    const PShape& sh = kShapes[i];
+    std::vector<float> w((size_t)sh.rows * sh.cols);
+    MLP_CUDA(cudaMemcpy(w.data(), *params_of(n, i), sizeof(float) * w.size(), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < sh.hrows; ++r)
+      for (int c = 0; c < sh.hcols; ++c) *dst++ = w[(size_t)r * sh.cols + c];
+  }
+  return LD_OK;
+}
+
+extern "C" ld_status ld_mlp_set_params(ld_mlp* n, const float* params) {
+  if (!n || !params) return ld_fail(LD_ERR_ARG, "null argument");
+  MLP_CUDA(cudaSetDevice(n->device));
+  const float* src = params;
+  for (int i = 0; i < 6; ++i) {
+    const PShape& sh = kShapes[i];
+    std::vector<float> w((size_t)sh.rows * sh.cols, 0.f);
+    for (int r = 0; r < sh.hrows; ++r)
+      for (int c = 0; c < sh.hcols; ++c) w[(size_t)r * sh.cols + c] = *src++;
+    MLP_CUDA(cudaMemcpy(*params_of(n, i), w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice));
+  }
+  MLP_CUDA(refresh_bf16(n));
+  MLP_CUDA(cudaStreamSynchronize(n->s));
+  return LD_OK;
+}
+
+extern "C" ld_status ld_mlp_forward(ld_mlp* n, const float* x, int32_t rows, float* logits) {
+  if (!n || !x || !logits || rows < 1) return ld_fail(LD_ERR_ARG, "bad arguments");
+  MLP_CUDA(cudaSetDevice(n->device));
+  std::vector<float> z((size_t)n->batch * kOutP);
+  for (int r0 = 0; r0 < rows; r0 += n->batch) {
+    const int cnt = std::min(n->batch, rows - r0);
+    ld_status st = upload_batch(n, x + (size_t)r0 * kIn, nullptr, nullptr, cnt);
+    if (st == LD_OK) st = forward(n);
+    if (st != LD_OK) return st;
+    MLP_CUDA(cudaMemcpyAsync(z.data(), n->Z3, sizeof(float) * z.size(), cudaMemcpyDeviceToHost, n->s));
+    st = check_err(n);
+    if (st != LD_OK) return st;
+    for (int r = 0; r < cnt; ++r) memcpy(logits + (size_t)(r0 + r) * kOut, &z[(size_t)r * kOutP], sizeof(float) * kOut);
+  }
+  return LD_OK;
+}
+
+// gradients of the mean masked BCE loss (flat host layout), no update
+extern "C" ld_status ld_mlp_gradients(ld_mlp* n, const float* x, const float* t, const float* mask, int32_t rows,
+                                      float* grads, float* loss) {
+  if (!n || !x || !t || !mask || rows < 1 || rows > n->batch) return ld_fail(LD_ERR_ARG, "bad arguments");
+  MLP_CUDA(cudaSetDevice(n->device));
+  double cnt = 0;
+  for (size_t i = 0; i < (size_t)rows * kOut; ++i) cnt += mask[i];
+  ld_status st = upload_batch(n, x, t, mask, rows);
+  if (st == LD_OK) st = forward(n);
+  if (st == LD_OK) st = backward(n, cnt > 0 ? (float)(1.0 / cnt) : 0.f);
+  if (st != LD_OK) return st;
+  st = check_err(n);
+  if (st != LD_OK) return st;
+  if (loss) MLP_CUDA(cudaMemcpy(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost));
+  if (grads) {
+    float* dst = grads;
+    for (int i = 0; i < 6; ++i) {
+      const PShape& sh = kShapes[i];
+      const int drows = i == 4 ? kOutGP : sh.rows;
+      std::vector<float> g((size_t)drows * sh.cols);
+      MLP_CUDA(cudaMemcpy(g.data(), *grads_of(n, i), sizeof(float) * g.size(), cudaMemcpyDeviceToHost));
+      for (int r = 0; r < sh.hrows; ++r)
+        for (int c = 0; c < sh.hcols; ++c) *dst++ = g[(size_t)r * sh.cols + c];
+    }
+  }
+  return LD_OK;
+}
+
+extern "C" ld_status ld_mlp_train_step(ld_mlp* n, const float* x, const float* t, const float* mask, int32_t rows,
+                                       float lr, float* loss) {
+  ld_status st = ld_mlp_gradients(n, x, t, mask, rows, nullptr, loss);
+  if (st != LD_OK) return st;
+  n->step += 1;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.f - std::pow(b1, (float)n->step), c2 = 1.f - std::pow(b2, (float)n->step);
+  for (int i = 0; i < 6; ++i) {
+    const PShape& sh = kShapes[i];
+    bf16* wb = i == 0 ? n->W1b : i == 2 ? n->W2b : i == 4 ? n->W3b : nullptr;
+    bf16* wbT = i == 2 ? n->W2T : i == 4 ? n->W3T : nullptr;
+    ld::mlp::adam_kernel<<<blocks_for(sh.rows * sh.cols), 256, 0, n->s>>>(
+        *params_of(n, i), *grads_of(n, i), n->m[i], n->v[i], sh.rows, sh.cols, lr, b1, b2, eps, c1, c2, wb, wbT);
+  }
+  MLP_CUDA(cudaGetLastError());
+  MLP_CUDA(cudaStreamSynchronize(n->s));
+  return LD_OK;
+}
+
+// Standalone tensor-core GEMM (bf16 bit patterns in, fp32 out) for tests:
+// C[M x N] = A[M x K] * B[N x K]^T, M % 128 == 0, N % 64 == 0, K % 64 == 0.
+extern "C" ld_status ld_tc_gemm(const uint16_t* A, const uint16_t* B, int32_t M, int32_t N, int32_t K, float* C,
+                                int32_t device) {
+  if (!A || !B || !C || M < 128 || M % 128 || N < 64 || N % 64 || K < 64 || K % 64)
+    return ld_fail(LD_ERR_ARG, "shape must be M%%128, N%%64, K%%64");
+  MLP_CUDA(cudaSetDevice(device));
+  void* mem = nullptr;
+  const size_t ba = (size_t)M * K * 2, bb = (size_t)N * K * 2, bc = (size_t)M * N * 4;
+  MLP_CUDA(cudaMalloc(&mem, ba + bb + bc + 256));
+  char* p = (char*)mem;
+  int* err = (int*)(p + ba + bb + bc);
+  cudaError_t e = cudaMemcpy(p, A, ba, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p + ba, B, bb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(err, 0, 4);
+  if (e == cudaSuccess)
+    e = gemm((const bf16*)p, (const bf16*)(p + ba), M, N, K, (float*)(p + ba + bb), nullptr, nullptr, nullptr, 0, err, 0);
+  int h_err = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(C, p + ba + bb, bc, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, 4, cudaMemcpyDeviceToHost);
+  cudaFree(mem);
+  if (e != cudaSuccess) return ld_fail(LD_ERR_CUDA, "tensor-core GEMM: %s", cudaGetErrorString(e));
+  if (h_err) return ld_fail(LD_ERR_TIMEOUT, "tensor-core GEMM wait ran out (code %d)", h_err);
+  return LD_OK;
+}
