@@ -262,8 +262,10 @@ void ld_batch_destroy(ld_batch *b);
 /* (0 drops an entry).  Parameters travel as one flat fp32 array: W1[256x44] */
 /* b1[256] W2[256x256] b2[256] W3[44x256] b3[44] (ld_mlp_param_count()).    */
 typedef struct ld_mlp ld_mlp;
-/* batch: rows per device pass, a positive multiple of 128. */
-ld_status ld_mlp_create(int32_t batch, uint64_t seed, int32_t device, ld_mlp **out);
+/* batch: rows per device pass, a positive multiple of 128.  skip: weight of
+ * a parameter-free residual path, logits = W3 h2 + b3 + skip * x (the
+ * input and output widths are equal; 0 turns it off). */
+ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int32_t device, ld_mlp **out);
 int64_t ld_mlp_param_count(void);
 ld_status ld_mlp_get_params(ld_mlp *net, float *params);
 ld_status ld_mlp_set_params(ld_mlp *net, const float *params);

@@ -101,7 +101,7 @@ SIGNATURES = [
     ("ld_plan_stream", C.c_void_p, [_P]),
     ("ld_plan_result_device", C.c_void_p, [_P]),
     ("ld_plan_destroy", None, [_P]),
-    ("ld_mlp_create", C.c_int, [C.c_int32, C.c_uint64, C.c_int32, C.POINTER(_P)]),
+    ("ld_mlp_create", C.c_int, [C.c_int32, C.c_uint64, C.c_float, C.c_int32, C.POINTER(_P)]),
     ("ld_mlp_param_count", C.c_int64, []),
     ("ld_mlp_get_params", C.c_int, [_P, _F32P]),
     ("ld_mlp_set_params", C.c_int, [_P, _F32P]),
@@ -501,11 +501,12 @@ class Mlp:
     """The proposal network on one GPU: forward, gradients and Adam steps run
     on the library's tensor-core kernels (bf16 operands, fp32 accumulate)."""
 
-    def __init__(self, batch: int = 1024, seed: int = 0, device: int = 0):
+    def __init__(self, batch: int = 1024, seed: int = 0, device: int = 0, skip: float = 0.0):
         h = C.c_void_p()
-        _check(lib().ld_mlp_create(int(batch), int(seed), int(device), C.byref(h)))
+        _check(lib().ld_mlp_create(int(batch), int(seed), float(skip), int(device), C.byref(h)))
         self._h = h
         self.batch = int(batch)
+        self.skip = float(skip)
 
     @staticmethod
     def param_count() -> int:

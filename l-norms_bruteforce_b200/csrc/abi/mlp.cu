@@ -54,6 +54,7 @@ int blocks_for(int n, int t = 256) { return (n + t - 1) / t; }
 
 struct ld_mlp {
   int device = 0, batch = 0;
+  float skip = 0.f;
   cudaStream_t s = nullptr;
   void* mem = nullptr;
   // fp32 master parameters (padded shapes), gradients, Adam moments
@@ -130,7 +131,11 @@ ld_status forward(ld_mlp* n) {
 ld_status backward(ld_mlp* n, float inv_count) {
   const int B = n->batch;
   MLP_CUDA(cudaMemsetAsync(n->loss, 0, sizeof(float), n->s));
+  // Xf and Z3 share the padded 64-column layout, so the residual input of
+  // output column c is input column c
+  static_assert(kInP == kOutP, "residual path needs equal padded widths");
   ld::mlp::bce_grad_kernel<<<blocks_for(B * kOutP), 256, 0, n->s>>>(n->Z3, n->Tt, n->Mk, B, kOutP, inv_count,
+                                                                     n->skip != 0.f ? n->Xf : nullptr, n->skip,
                                                                      n->dZ3, n->dZ3T, n->loss);
   MLP_CUDA(cudaGetLastError());
   // W3: [kOutGP x B] x [kHid x B]^T (rows kOutP.. of dZ3T are zero)
@@ -163,12 +168,13 @@ ld_status check_err(ld_mlp* n) {
 
 }  // namespace
 
-extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, int32_t device, ld_mlp** out) {
+extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int32_t device, ld_mlp** out) {
   if (!out || batch < 128 || batch % 128) return ld_fail(LD_ERR_ARG, "batch must be a positive multiple of 128");
   if (cudaSetDevice(device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "no device %d", device);
   ld_mlp* n = new ld_mlp();
   n->device = device;
   n->batch = batch;
+  n->skip = skip;
   const int B = batch;
   // one allocation, carved in 256-byte aligned pieces
   struct Piece { void** p; size_t bytes; };
@@ -275,7 +281,9 @@ extern "C" ld_status ld_mlp_forward(ld_mlp* n, const float* x, int32_t rows, flo
     MLP_CUDA(cudaMemcpyAsync(z.data(), n->Z3, sizeof(float) * z.size(), cudaMemcpyDeviceToHost, n->s));
     st = check_err(n);
     if (st != LD_OK) return st;
-    for (int r = 0; r < cnt; ++r) memcpy(logits + (size_t)(r0 + r) * kOut, &z[(size_t)r * kOutP], sizeof(float) * kOut);
+    for (int r = 0; r < cnt; ++r)
+      for (int c = 0; c < kOut; ++c)
+        logits[(size_t)(r0 + r) * kOut + c] = z[(size_t)r * kOutP + c] + n->skip * x[(size_t)(r0 + r) * kIn + c];
   }
   return LD_OK;
 }

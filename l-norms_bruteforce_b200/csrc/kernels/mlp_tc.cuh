@@ -198,14 +198,17 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(const GemmArgs g) {
 // ---- element-wise parts ---------------------------------------------------
 
 // BCE with logits over valid entries: dz = (sigmoid(z) - t) * mask / count,
-// written as bf16 (row-major and transposed); loss accumulated.
+// written as bf16 (row-major and transposed); loss accumulated.  The logit
+// is the network output plus `skip` times the input of the same index
+// (a residual path without parameters; skip_x may be null).
 __global__ void bce_grad_kernel(const float* z, const float* t, const float* mask, int rows, int cols,
-                                float inv_count, __nv_bfloat16* dz, __nv_bfloat16* dzT, float* loss) {
+                                float inv_count, const float* skip_x, float skip, __nv_bfloat16* dz,
+                                __nv_bfloat16* dzT, float* loss) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float l = 0.f;
   if (i < rows * cols) {
     const int r = i / cols, c = i % cols;
-    const float x = z[i], m = mask[i], y = t[i];
+    const float x = z[i] + (skip_x ? skip * skip_x[i] : 0.f), m = mask[i], y = t[i];
     const float s = 1.f / (1.f + expf(-x));
     const float g = (s - y) * m * inv_count;
     dz[i] = __float2bfloat16_rn(g);

@@ -8,7 +8,8 @@ forward and backward passes here round at exactly the points the device
 kernels round (inputs, weights, hidden activations, and the gradients that
 feed GEMMs) and accumulate in float64, so the device results must agree up
 to fp32 accumulation order and the occasional one-ulp bf16 rounding flip.
-`exact=True` turns every rounding off (plain float64 backpropagation),
+`skip` is the weight of the parameter-free residual path (logit += skip *
+input of the same index).  `exact=True` turns every rounding off (plain float64 backpropagation),
 which the tests check against finite differences.
 
 Only tests import this module; the product path never does.
@@ -38,25 +39,25 @@ def _r(x, exact):
     return np.asarray(x, dtype=np.float64) if exact else bf16(x)
 
 
-def forward(p: dict, x, exact: bool = False):
-    """Logits and the cached activations."""
+def forward(p: dict, x, exact: bool = False, skip: float = 0.0):
+    """Logits (network output + skip * x) and the cached activations."""
     X = _r(x, exact)
     W1, W2, W3 = (_r(p[k], exact) for k in ("W1", "W2", "W3"))
     Z1 = X @ W1.T + p["b1"]
     H1 = _r(np.maximum(Z1, 0), exact)
     Z2 = H1 @ W2.T + p["b2"]
     H2 = _r(np.maximum(Z2, 0), exact)
-    Z3 = H2 @ W3.T + p["b3"]
+    Z3 = H2 @ W3.T + p["b3"] + skip * np.asarray(x, dtype=np.float64)
     return Z3, dict(X=X, H1=H1, H2=H2, W2=W2, W3=W3)
 
 
-def loss_and_grads(p: dict, x, t, mask, exact: bool = False):
+def loss_and_grads(p: dict, x, t, mask, exact: bool = False, skip: float = 0.0):
     """Mean masked BCE-with-logits and its gradients (same keys as p)."""
     t = np.asarray(t, dtype=np.float64)
     m = np.asarray(mask, dtype=np.float64)
     cnt = m.sum()
     inv = 1.0 / cnt if cnt > 0 else 0.0
-    Z3, c = forward(p, x, exact)
+    Z3, c = forward(p, x, exact, skip)
     loss = float((m * (np.maximum(Z3, 0) - Z3 * t + np.log1p(np.exp(-np.abs(Z3))))).sum() * inv)
     s = 1.0 / (1.0 + np.exp(-Z3))
     dZ3 = _r((s - t) * m * inv, exact)

@@ -1,0 +1,99 @@
+"""Learned-pruned search on the GPU.
+
+Exactness: whatever the proposals, the learned pipeline returns the plain
+enumeration's value and Gray index.  Gain: with the same number of
+proposals, the trained network's incumbents are compared with the method
+without it (uniform random starts, and the spectral sign starts the network
+refines), on held-out matrices of the training distribution and on the
+44 x 44 low-rank workload."""
+import json
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def L(ld):
+    import lnorms_b200.learned as L
+    return L
+
+
+@pytest.fixture(scope="module")
+def trained(L):
+    if not L.WEIGHTS.exists():
+        pytest.fail(f"trained weights missing: {L.WEIGHTS}")
+    with np.load(L.WEIGHTS) as f:
+        return {k: f[k] for k in f.files}
+
+
+@pytest.mark.parametrize("mode", ["random", "spectral", "network"])
+def test_learned_equals_plain(ld, L, workloads, trained, mode):
+    rng = np.random.default_rng(21)
+    p = L.Proposer(mode, directions=8, samples=2, params=trained if mode == "network" else None)
+    for n in (8, 17, 23, 26):
+        a = workloads.lowrank(n, 44, rng)
+        plain = ld.solve_reduced(a, 1)
+        sol, st = L.solve_learned(a, p)
+        assert (sol.value, sol.gray_index) == (plain.value, plain.gray_index)
+        assert st["incumbent"] <= plain.value
+    p.close()
+
+
+def test_learned_exact_with_untrained_network(ld, L, workloads):
+    """A network that has learned nothing still gives the exact answer."""
+    rng = np.random.default_rng(22)
+    net = ld.Mlp(batch=128, seed=9)
+    params = net.get_params()
+    net.close()
+    params["skip"] = 0.0
+    p = L.Proposer("network", directions=8, samples=1, params=params)
+    for n in (12, 24):
+        a = workloads.lowrank(n, 44, rng)
+        plain = ld.solve_reduced(a, 1)
+        sol, _ = L.solve_learned(a, p)
+        assert (sol.value, sol.gray_index) == (plain.value, plain.gray_index)
+    p.close()
+
+
+def _modes(L, trained, directions, samples):
+    return [L.Proposer(mode, directions=directions, samples=samples,
+                       params=trained if mode == "network" else None) for mode in L.PROPOSAL_MODES]
+
+
+def test_network_gain_on_heldout(ld, L, workloads, trained):
+    hold = workloads.config5_training(48, seed=57)
+    _, opt, _ = L.solve_training_set(hold)
+    rows = {}
+    for directions in (4, 8, 32):
+        for p in _modes(L, trained, directions, 1):
+            r = L.evaluate(hold, opt, p)
+            rows[(p.mode, directions)] = r
+            p.close()
+    print("\nheld-out incumbents (48 matrices, n in [16, 28], 44 columns):")
+    for r in rows.values():
+        print(json.dumps(r))
+    for directions in (4, 8, 32):
+        net, rnd = rows[("network", directions)], rows[("random", directions)]
+        # the trained network's raw proposals are far better than uniform ones
+        assert net["raw_best_ratio"] > rnd["raw_best_ratio"] + 0.2
+    assert rows[("network", 32)]["optimal_rate"] >= 0.95
+
+
+def test_network_gain_on_lowrank_44(ld, L, workloads, trained):
+    inst = workloads.config5()
+    a = inst.matrix
+    out = {}
+    for p in _modes(L, trained, 8, 1):
+        sol, st = L.solve_learned(a, p)
+        out[p.mode] = (sol, st)
+        p.close()
+    print("\n44 x 44 low-rank, 8 proposals per mode:")
+    for mode, (sol, st) in out.items():
+        print(mode, json.dumps({k: st[k] for k in ("incumbent", "raw_best", "polished_mean", "incumbent_s",
+                                                   "pruned_s", "total_s", "prune_scan_ms")}))
+    ref = out["random"][0]
+    for mode, (sol, _) in out.items():
+        assert (sol.value, sol.gray_index) == (ref.value, ref.gray_index) == (7023, 7492441473292)
+    assert out["network"][1]["raw_best"] > out["random"][1]["raw_best"]
