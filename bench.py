@@ -54,53 +54,121 @@ def instance(cfg: int):
 
 
 def ops_per_labeling(d: int, cols: int) -> int:
-    """Algorithmic integer work per labeling: update + |.| + accumulate per
-    column (3m) for L_1/LM; two changed message vectors (6m) for d >= 2."""
+    """Integer work per labeling of the plain incremental method: update +
+    |.| + accumulate per column (3m) for L_1/LM; two changed message vectors
+    (6m) for d >= 2."""
     return 3 * cols if d == 1 else 6 * cols
+
+
+def issue_ops_per_labeling(desc: str, d: int, cols: int) -> tuple[int, str]:
+    """int32 ALU issue slots the chosen kernel spends per labeling.
+
+    Table kernel: one absolute-difference-accumulate instruction (sad on a
+    32-bit lane, vabsdiff4 on four 8-bit lanes) per column word per sum
+    vector (D vectors per labeling: 1 for L_1/LM, 2 or 3 for d = 2, 3); both
+    issue at half the ALU pipe's add/xor rate, so each costs 2 slots of the
+    int32 add/xor peak.  Wide kernel: the plain count."""
+    f = dict(kv.split("=") for kv in desc.replace("int32 words", "int32_words")
+             .replace("int8x4 words", "int8x4_words").split() if "=" in kv)
+    if desc.startswith("table") and "int32_words" in f:
+        D, wb, wa = int(f["D"]), int(f["int32_words"]), int(f["int8x4_words"])
+        return 2 * D * (wb + wa), f"2 slots x D={D} x ({wb} int32 + {wa} int8x4 words)"
+    return ops_per_labeling(d, cols), "plain count (wide kernel)"
+
+
+# DRAM traffic of one launch of the config-2 table kernel, from the ncu
+# capture summarised in profiles/table_kernel_config2_LM_34x37.md
+# (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is ALU-bound and
+# reads only its matrix image.
+TRAFFIC_BYTES = {2: 36608}
 
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled every 10 ms through NVML (read
+    only) while the timed region runs; falls back to `nvidia-smi -lms 200`."""
 
-    def __init__(self, index: int):
-        self.index = index
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, index: int, interval: float = 0.01):
+        import threading
+        self.samples, self.reasons = [], set()
+        self.sm_max = None
+        self.proc = None
+        self._stop = threading.Event()
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(index)
+            self.sm_max = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            get_reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                N.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def loop():
+                while not self._stop.is_set():
+                    self.samples.append(float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)))
+                    r = get_reasons(h)
+                    for nm, bit in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(nm)
+                    self._stop.wait(interval)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            while not self.samples and self.thread.is_alive():
+                time.sleep(0.001)
+        except Exception:
+            self.thread = None
+            self._start_smi(index)
+
+    def _start_smi(self, index):
+        fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={fields}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.file.flush()
-        rows = [ln.split(",") for ln in Path(self.file.name).read_text().splitlines() if ln.strip()]
-        os.unlink(self.file.name)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
+            sm = self.samples
+            smax = [self.sm_max] if self.sm_max else sm
+            reasons = self.reasons
+            source = "nvml 10 ms"
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(r[1])); smax.append(float(r[2]))
-            except (ValueError, IndexError):
-                continue
-            for nm, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(nm)
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.file.flush()
+            rows = [ln.split(",") for ln in Path(self.file.name).read_text().splitlines() if ln.strip()]
+            os.unlink(self.file.name)
+            sm, smax, reasons = [], [], set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                try:
+                    sm.append(float(r[1])); smax.append(float(r[2]))
+                except (ValueError, IndexError):
+                    continue
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            source = "nvidia-smi 200 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
         loaded = [s for s in sm if s >= 0.5 * max(sm)] or sm
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": source}
 
 
 # ---------------------------------------------------------------- CPU side
@@ -326,9 +394,12 @@ def run_ours(args) -> None:
 
     if rank == 0:
         kernel_ms = statistics.mean(step_ms)
+        desc = plan.describe()
         opl = ops_per_labeling(d, info["cols"])
+        iopl, iwhat = issue_ops_per_labeling(desc, d, info["cols"])
         peak_ops, _ = ld.int32_peak(local)
-        achieved = opl * (hi - lo) / (kernel_ms * 1e-3)
+        rate = (hi - lo) / (kernel_ms * 1e-3)
+        achieved = iopl * rate
         line = {
             "metric": "exact L_d labelings/s (plain enumeration)", "value": value, "unit": "labelings/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -338,11 +409,17 @@ def run_ours(args) -> None:
                        "d": d, "marginal": marg, "labelings_per_step": total_labelings,
                        "parallelism": f"gray-index shards x{world}" if world > 1 else "single GPU",
                        "l2": "flushed between steps (512 MiB write outside the timed events)",
-                       "kernel": plan.describe(), "value": sol.value, "gray_index": sol.gray_index},
+                       "kernel": desc, "value": sol.value, "gray_index": sol.gray_index},
             "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12,
-                         "unit": "Tops/s", "frac": achieved / peak_ops, "traffic": None,
-                         "note": f"{opl} algorithmic int32 ops per labeling ({'3m' if d == 1 else '6m'}, "
-                                 f"m={info['cols']}); peak = int32 add/xor microbenchmark measured in this run"},
+                         "unit": "Tops/s", "frac": achieved / peak_ops,
+                         "traffic": TRAFFIC_BYTES.get(args.config) if world == 1 else None,
+                         "ops_per_labeling": iopl,
+                         "plain_method": {"ops_per_labeling": opl, "achieved": opl * rate / 1e12,
+                                          "x_peak": opl * rate / peak_ops},
+                         "note": f"achieved = {iopl} int32 issue slots per labeling ({iwhat}) x labelings/s; "
+                                 f"peak = int32 add/xor microbenchmark measured in this run; plain_method "
+                                 f"counts the {'3m' if d == 1 else '6m'} ops the plain enumeration spends per "
+                                 f"labeling (m={info['cols']}), which the table decomposition avoids"},
             "e2e": {"value": e2e_value, "unit": "labelings/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": statistics.mean(e2e_ms)},
             "gpu_launches": args.steps,
