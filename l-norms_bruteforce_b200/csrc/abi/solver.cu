@@ -229,7 +229,7 @@ struct Resources {
   size_t hcap = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };
 
 void resources_release(Resources* r) {
@@ -242,6 +242,7 @@ void resources_release(Resources* r) {
   if (r->hstage) cudaFreeHost(r->hstage);
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
+  if (r->ev2) cudaEventDestroy(r->ev2);
   if (r->own_stream && r->stream) cudaStreamDestroy(r->stream);
   if (cur >= 0) cudaSetDevice(cur);
   *r = Resources();
@@ -256,6 +257,7 @@ ld_status resources_acquire(Resources* r, int device, cudaStream_t user_stream, 
     else { LD_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking)); r->own_stream = true; }
     LD_CUDA(cudaEventCreate(&r->ev0));
     LD_CUDA(cudaEventCreate(&r->ev1));
+    LD_CUDA(cudaEventCreate(&r->ev2));
   }
   if (r->dcap < dbytes) {
     if (r->dmem) { LD_CUDA(cudaStreamSynchronize(r->stream)); LD_CUDA(cudaFree(r->dmem)); r->dmem = nullptr; r->dcap = 0; }
@@ -272,6 +274,10 @@ ld_status resources_acquire(Resources* r, int device, cudaStream_t user_stream, 
 
 std::mutex g_ws_mu[64];
 Resources g_ws[64];
+// per-device workspace of the pruned search (its own stream, arena and
+// pinned result staging), kept between calls
+std::mutex g_pws_mu[64];
+Resources g_pws[64];
 
 constexpr size_t kOffCounter = 0, kOffGvalue = 8, kOffResult = 16;
 constexpr size_t kOffTot = 256, kOffH0 = 512, kOffTb = 768, kOffA = 1024;
@@ -770,26 +776,25 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
   const size_t off_list = off_slots + align256(blocks_s * sizeof(ld::Slot));
   const size_t off_cnt = off_list + align256(walks * 8);
   const size_t dbytes = off_cnt + 256;
-  char* dmem = nullptr;
-  cudaStream_t s = (cudaStream_t)o.stream;
-  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-  ld::Slot out{};
-  unsigned long long hstat[4] = {0, 0, 0, 0};
+  if (o.device < 0 || o.device >= 64) return ld_fail(LD_ERR_ARG, "device %d out of range", o.device);
+  std::lock_guard<std::mutex> lock(g_pws_mu[o.device]);
+  Resources* r = &g_pws[o.device];
+  // the workspace keeps the stream it was created with: the caller's, or its own
+  if (r->device >= 0 && (cudaStream_t)o.stream != (r->own_stream ? nullptr : r->stream)) resources_release(r);
+  st = resources_acquire(r, o.device, (cudaStream_t)o.stream, dbytes, 256);
+  if (st != LD_OK) return st;
+  char* dmem = (char*)r->dmem;
+  cudaStream_t s = r->stream;
+  ld::Slot* out_h = (ld::Slot*)r->hstage;
+  unsigned long long* hstat = (unsigned long long*)((char*)r->hstage + 64);
   float ms_b = 0.f, ms_s = 0.f;
   auto fail = [&](const char* what, cudaError_t e) {
-    if (dmem) cudaFree(dmem);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    if (e2) cudaEventDestroy(e2);
+    cudaStreamSynchronize(s);
     return ld_fail(LD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   };
-  cudaError_t e = cudaMalloc(&dmem, dbytes);
-  if (e != cudaSuccess) return fail("cudaMalloc", e);
+  cudaError_t e;
   if ((e = cudaMemsetAsync(dmem + off_cnt, 0, 256, s)) != cudaSuccess) return fail("memset", e);
   if ((e = cudaMemcpyAsync(dmem, image.data(), upload, cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload", e);
-  if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess ||
-      (e = cudaEventCreate(&e2)) != cudaSuccess)
-    return fail("events", e);
   {
     ld::PruneArgs args;
     ld::TableArgs& t = args.t;
@@ -813,21 +818,22 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     args.list_count = (unsigned long long*)(dmem + off_cnt);
     args.stats = (unsigned long long*)(dmem + off_cnt + 8);
     void* params[] = {&args};
-    if ((e = cudaEventRecord(e0, s)) != cudaSuccess) return fail("event", e);
+    if ((e = cudaEventRecord(r->ev0, s)) != cudaSuccess) return fail("event", e);
     if ((e = cudaLaunchKernel(kb, dim3((unsigned)blocks_b), dim3(ld::kPruneThreads), params, smem_b, s)) != cudaSuccess)
       return fail("walk bound launch", e);
-    if ((e = cudaEventRecord(e1, s)) != cudaSuccess) return fail("event", e);
+    if ((e = cudaEventRecord(r->ev1, s)) != cudaSuccess) return fail("event", e);
     if ((e = cudaLaunchKernel(ks, dim3((unsigned)blocks_s), dim3(ld::kPruneThreads), params, smem_s, s)) != cudaSuccess)
       return fail("scan launch", e);
-    if ((e = cudaEventRecord(e2, s)) != cudaSuccess) return fail("event", e);
+    if ((e = cudaEventRecord(r->ev2, s)) != cudaSuccess) return fail("event", e);
   }
-  if ((e = cudaMemcpyAsync(&out, dmem + 16, sizeof out, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return fail("result", e);
-  if ((e = cudaMemcpyAsync(hstat, dmem + off_cnt, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return fail("stats", e);
+  if ((e = cudaMemcpyAsync(out_h, dmem + 16, sizeof(ld::Slot), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return fail("result", e);
+  if ((e = cudaMemcpyAsync(hstat, dmem + off_cnt, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return fail("stats", e);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail("solve", e);
-  cudaEventElapsedTime(&ms_b, e0, e1);
-  cudaEventElapsedTime(&ms_s, e1, e2);
-  cudaFree(dmem);
-  cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+  cudaEventElapsedTime(&ms_b, r->ev0, r->ev1);
+  cudaEventElapsedTime(&ms_s, r->ev1, r->ev2);
+  const ld::Slot out = *out_h;
   if (ps.incumbent != LLONG_MIN && out.value < ps.incumbent)
     return ld_fail(LD_ERR_CUDA, "internal: pruned result %lld below the incumbent %lld", (long long)out.value,
                    (long long)ps.incumbent);
@@ -839,7 +845,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
   res->kernel_kind = LD_KERNEL_TABLE;
   res->lane_bits = ch.lane_bits;
   res->h2d_bytes = upload;
-  res->d2h_bytes = sizeof out + sizeof hstat;
+  res->d2h_bytes = sizeof out + 4 * sizeof(unsigned long long);
   if (strategy) ld_gray_labels(out.index, R, d, strategy);
   ps.pruned = 1;
   ps.walks_kept = hstat[1];

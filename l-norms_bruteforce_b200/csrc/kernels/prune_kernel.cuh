@@ -219,6 +219,11 @@ __host__ __device__ inline int prune_smem_words(int D, int W, int R, int B, bool
 }
 
 // Launch 1: bound every walk's top-row prefix; list the walks that survive.
+// Each thread takes a contiguous run of walk indices and visits them in
+// order: the top rows' labels are the reflected Gray code of the walk index
+// (binary for d <= 2, 3-ary for d = 3), so consecutive walks differ in one
+// top row, and the prefix vector is seeded once per run and then updated by
+// one row move per walk.
 template <int D, int WB, int WA>
 __global__ void __launch_bounds__(kPruneThreads) walk_bound_kernel(const PruneArgs args) {
   using S = Shape<D, WB, WA>;
@@ -235,13 +240,33 @@ __global__ void __launch_bounds__(kPruneThreads) walk_bound_kernel(const PruneAr
   unsigned long long kept = 0;
   // every lane of a warp runs the same number of iterations (ballots below)
   const unsigned long long nw = ta.walk_end - ta.walk_begin;
-  const unsigned long long rounds = (nw + T - 1) / T;
+  const unsigned long long run = (nw + T - 1) / T;
+  const unsigned long long first = ta.walk_begin + tid * run;
   uint32_t H[S::NR * S::WV];
-  for (unsigned long long r = 0; r < rounds; ++r) {
-    const unsigned long long wk = ta.walk_begin + tid + r * T;
+  for (unsigned long long r = 0; r < run; ++r) {
+    const unsigned long long wk = first + r;
     bool keep = false;
     if (wk < ta.walk_end) {
-      seed_top<D, WB, WA>(H, sA, sH0, k, fw, nh, wk * ta.walk_len);
+      if (r == 0) {
+        seed_top<D, WB, WA>(H, sA, sH0, k, fw, nh, wk * ta.walk_len);
+      } else {
+        // the one top row whose label differs between walks wk - 1 and wk
+        int i, a, b;
+        if (D <= 2) {
+          i = __ffsll((long long)wk) - 1;
+          b = (int)(((wk >> (i + 1)) & 1ull) ^ 1ull);
+          a = b ^ 1;
+        } else {
+          unsigned long long q = wk;
+          i = 0;
+          while (q % 3ull == 0ull) { q /= 3ull; ++i; }
+          const int c = (int)(q % 3ull);
+          const int par = (int)((q / 3ull) & 1ull);
+          b = par ? 2 - c : c;
+          a = par ? 3 - c : c - 1;
+        }
+        move_row<D, WB, WA>(H, sA + (k + fw + i) * S::WT, a, b);
+      }
       keep = prefix_abs<D, WB, WA>(H, sTtop) + args.m_walk >= args.threshold;
     }
     const unsigned mask = __ballot_sync(0xffffffffu, keep);
@@ -275,23 +300,36 @@ __global__ void __launch_bounds__(kPruneThreads) prune_scan_kernel(const PruneAr
   const int lane = threadIdx.x & 31;
   const unsigned long long WL = ta.walk_len;
   const unsigned long long nlist = *args.list_count;
-  const unsigned long long rounds = (nlist + T - 1) / T;
+  // Few surviving walks would leave most threads idle, so each walk is cut
+  // into `split` parts of PL consecutive high indices (at least 8 each), one
+  // part per thread; every part is seeded directly and then walked.
+  unsigned long long split = nlist ? T / nlist : 1ull;
+  const unsigned long long max_split = WL >= 16ull ? WL / 8ull : 1ull;
+  split = split < 1ull ? 1ull : (split > max_split ? max_split : split);
+  const unsigned long long PL = (WL + split - 1) / split;
+  const unsigned long long items = nlist * split;
+  const unsigned long long rounds = (items + T - 1) / T;
   long long bv = LLONG_MIN;
   unsigned long long bn = ULLONG_MAX;
   unsigned long long hk = 0, hv = 0;
   uint32_t H[NREG];
   for (unsigned long long r = 0; r < rounds; ++r) {
-    const unsigned long long slot = tid + r * T;
-    const bool live = slot < nlist;
+    const unsigned long long item = tid + r * T;
+    const unsigned long long slot = item / split, part = item % split;
+    const unsigned long long u0 = part * PL;
+    const bool live = item < items && u0 < WL;
     const unsigned long long wk = live ? args.list[slot] : 0ull;
     const unsigned long long h0 = wk * WL;
+    const unsigned long long u1 = live ? (u0 + PL < WL ? u0 + PL : WL) : 0ull;
     if (live) {
       seed_top<D, WB, WA>(H, sA, sH0, k, fw, nh, h0);
-      add_walk_rows<D, WB, WA>(H, sA, k, fw, h0);
+      add_walk_rows<D, WB, WA>(H, sA, k, fw, h0 + u0);
     }
-    for (unsigned long long u = 0; u < WL; ++u) {
+    for (unsigned long long uu = 0; uu < PL; ++uu) {
+      const unsigned long long u = u0 + uu;
+      const bool on = live && u < u1;
       const unsigned long long h = h0 + u;
-      if (live && u) {
+      if (on && uu) {
         int i, a, b;
         if (D <= 2) {
           i = __ffsll((long long)u) - 1;
@@ -308,8 +346,8 @@ __global__ void __launch_bounds__(kPruneThreads) prune_scan_kernel(const PruneAr
         }
         move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
       }
-      const bool scan = live && prefix_abs<D, WB, WA>(H, sThigh) + args.m_low >= args.threshold;
-      hv += live ? 1ull : 0ull;
+      const bool scan = on && prefix_abs<D, WB, WA>(H, sThigh) + args.m_low >= args.threshold;
+      hv += on ? 1ull : 0ull;
       hk += scan ? 1ull : 0ull;
       unsigned mask = __ballot_sync(0xffffffffu, scan);
       while (mask) {
