@@ -711,8 +711,11 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
   }
   if (k < 0) return plain();
   const int nh = F - k;
+  // walk rows: every walk gets one bound in the first launch, so at most
+  // about 2^21 walks; the surviving walks' high indices are split over the
+  // threads of the scan, so long walks cost nothing extra there
   int fw = std::min(nh, 5);
-  while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 26.0) ++fw;
+  while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 21.0) ++fw;
   const unsigned long long walk_len = ipow(base, fw), walks = ipow(base, nh - fw);
   const int B = (int)ipow(base, k);
   ps.low_rows = k; ps.walk_rows = fw;
