@@ -67,11 +67,15 @@ def issue_ops_per_labeling(desc: str, d: int, cols: int) -> tuple[int, str]:
     32-bit lane, vabsdiff4 on four 8-bit lanes) per column word per sum
     vector (D vectors per labeling: 1 for L_1/LM, 2 or 3 for d = 2, 3); both
     issue at half the ALU pipe's add/xor rate, so each costs 2 slots of the
-    int32 add/xor peak.  Wide kernel: the plain count."""
+    int32 add/xor peak.  The LM instances that add the marginal column
+    linearly skip its word.  Wide kernel: the plain count."""
     f = dict(kv.split("=") for kv in desc.replace("int32 words", "int32_words")
              .replace("int8x4 words", "int8x4_words").split() if "=" in kv)
     if desc.startswith("table") and "int32_words" in f:
         D, wb, wa = int(f["D"]), int(f["int32_words"]), int(f["int8x4_words"])
+        if int(f.get("lin", 0)):
+            # the LM marginal column is added linearly, once per high index
+            return 2 * (D * (wb + wa) - 1), f"2 slots x ({wb - 1} int32 + {wa} int8x4 words; column 0 linear)"
         return 2 * D * (wb + wa), f"2 slots x D={D} x ({wb} int32 + {wa} int8x4 words)"
     return ops_per_labeling(d, cols), "plain count (wide kernel)"
 
@@ -454,7 +458,7 @@ def run_batch(args) -> None:
     torch.cuda.set_device(local)
     ld = load_package()
     import lnorms_b200.workloads as W
-    mats, ds, skipped, skipped_lab, total = [], [], 0, 0, 0
+    mats, ds, skipped, skipped_lab, total, slots = [], [], 0, 0, 0, 0
     for inst in W.config4():
         p = ld.Problem.from_matrix(inst.matrix, inst.d)
         info = p.info
@@ -465,6 +469,9 @@ def run_batch(args) -> None:
         mats.append(p.reduced)
         ds.append(info["d"])
         total += int(info["labelings"])
+        # int32 issue slots per labeling: one sad (2 slots) per column per
+        # sum vector (all of this workload's sums need 32-bit lanes)
+        slots += 2 * info["d"] * info["cols"] * int(info["labelings"])
     opts = ld.options(device=local)
     t0 = time.perf_counter()
     b = ld.Batch(mats, ds, opts=opts, autotune=True)
@@ -494,6 +501,8 @@ def run_batch(args) -> None:
         return
     dev_s = sum(ms) * 1e-3
     h2d = sum(m.size * 8 for m in mats)
+    peak_ops, _ = ld.int32_peak(local)
+    achieved = slots * args.steps / dev_s
     line = {
         "metric": "exact L_d labelings/s (batched solves)", "value": total * args.steps / dev_s,
         "unit": "labelings/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -507,7 +516,14 @@ def run_batch(args) -> None:
                    "l2": "not flushed: the batch's inputs are a few MB and stay resident"},
         "e2e": {"value": total / statistics.mean(e2e), "unit": "labelings/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": len(mats) * 16, "s_per_step": statistics.mean(e2e)},
-        "roofline": None,
+        "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "Tops/s",
+                     "frac": achieved / peak_ops, "traffic": None, "ops_per_labeling": slots / total,
+                     "note": "2 int32 issue slots (one sad) per column per sum vector per labeling, unpadded "
+                             "columns, averaged over the batch; peak = int32 add/xor microbenchmark measured "
+                             "in this run"},
+        # per replay: one persistent kernel per lane class, the fold, and the own plans' kernels
+        "gpu_launches": len(ms) * (int(desc.split(" classes")[0].split()[-1]) + 1
+                                   + int(desc.split(" own plans")[0].split()[-1])),
         "clocks": clk,
     }
     print(json.dumps(line))

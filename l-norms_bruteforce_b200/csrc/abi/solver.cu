@@ -70,6 +70,7 @@ struct Choice {
   std::vector<int> order;                     // table: column of each lane (wide first)
   int PC = 0, multi = 0, i64 = 0;             // wide
   int lane_bits = 0;
+  int lin = 0;                                // table: LM column 0 linear in word 0
 };
 
 int round4(int x) { return (x + 3) & ~3; }
@@ -374,6 +375,11 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     const int D = p->ch.D, WT = p->ch.WT;
     p->kfn = ld::table_kernel_mixed_ptr(D, p->ch.WB, p->ch.WA);
     if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no table kernel for D=%d WB=%d WA=%d", D, p->ch.WB, p->ch.WA); }
+    // LM with the marginal column in a 32-bit word of its own: its term is
+    // never negative, so the instance that adds it linearly applies
+    if (D == 1 && marginal && p->ch.WB >= 1 && !p->ch.order.empty() && p->ch.order[0] == 0) {
+      if (const void* lk = ld::table_kernel_lin_ptr(p->ch.WB, p->ch.WA)) { p->kfn = lk; p->ch.lin = 1; }
+    }
     const int k = p->ch.k;
     p->k = k;
     p->B = (int)ipow(base, k);
@@ -566,8 +572,8 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (!p || !buf) return ld_fail(LD_ERR_ARG, "null argument");
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
-             "table D=%d int32 words=%d int8x4 words=%d k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d smem=%zu",
-             p->ch.D, p->ch.WB, p->ch.WA, p->k, p->B, p->fw,
+             "table D=%d int32 words=%d int8x4 words=%d lin=%d k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d smem=%zu",
+             p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->k, p->B, p->fw,
              (unsigned long long)p->walks, p->blocks, p->tpb, p->smem);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d", p->ch.PC, p->ch.multi,

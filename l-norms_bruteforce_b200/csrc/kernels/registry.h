@@ -16,8 +16,14 @@ void table_register_d1_p32b(TableKernelTab& t);
 void table_register_d2(TableKernelTab& t);
 void table_register_d3(TableKernelTab& t);
 
+// table_kernel<1, WB, WA, true> (LM, marginal column linear in word 0) by
+// (WB, WA): WB in 1..2, WA in 0..16
+using TableKernelLinTab = const void* [3][17];
+void table_register_d1_lin(TableKernelLinTab& t);
+
 // nullptr when not instantiated
 const void* table_kernel_mixed_ptr(int D, int WB, int WA);
+const void* table_kernel_lin_ptr(int WB, int WA);
 // all columns in one lane width: PK = 1 (int32, W words) or 4 (int8x4, W words)
 const void* table_kernel_ptr(int D, int W, int PK);
 // pruned-search kernels {walk_bound_kernel, prune_scan_kernel} for (D, WB, WA):

@@ -36,7 +36,11 @@
 // LM enters as L_1 with column 0 shifted by K = sum_i |A_i0|: K_H (the
 // high and fixed rows' share) is added to H's column 0 and K_L (the low
 // rows' share) is subtracted through the table bias tb, so that column's
-// term is its signed sum plus K; K is subtracted from the result.
+// term is its signed sum plus K; K is subtracted from the result.  When
+// column 0 has a 32-bit lane of its own (word 0), the LIN instances use that
+// its term needs no absolute value: the table stores its negation as the
+// accumulator's starting value and H's column 0 is added once per high
+// index, which saves one instruction per labeling.
 #pragma once
 #include "common.cuh"
 
@@ -170,10 +174,14 @@ __device__ __forceinline__ constexpr bool computed(int q) {
   return q % S::WT < S::WV;
 }
 
-// acc += |H - e| over the words of x (table words 4q .. 4q+3)
-template <int D, int WB, int WA>
+// acc += |H - e| over the words of x (table words 4q .. 4q+3).  LIN: word 0
+// is a column that enters the value linearly (the LM marginal column, whose
+// term H_0 - e_0 is never negative); its table word holds -e_0, which only
+// seeds the accumulator, and H_0 is added once per high index by the caller.
+template <int D, int WB, int WA, bool LIN = false>
 __device__ __forceinline__ void sad4(const uint32_t* H, const uint4& x, int q, uint32_t& a0, uint32_t& a1) {
   using S = Shape<D, WB, WA>;
+  static_assert(!LIN || (D == 1 && WB >= 1), "the linear column is a 32-bit word of an L_1 vector");
   const uint32_t xs[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
@@ -181,7 +189,9 @@ __device__ __forceinline__ void sad4(const uint32_t* H, const uint4& x, int q, u
     if (computed<D, WB, WA>(tq)) {
       uint32_t& acc = (c & 1) ? a1 : a0;
       const int w = tq % S::WT;
-      if (D == 3 && S::NR == 2 && tq / S::WT == 2)   // H1 + H2, formed on the fly
+      if (LIN && tq == 0)
+        acc += xs[c];
+      else if (D == 3 && S::NR == 2 && tq / S::WT == 2)   // H1 + H2, formed on the fly
         acc = wsad<WB>(w, wadd<WB>(w, H[w], H[S::WV + w]), xs[c], acc);
       else
         acc = wsad<WB>(w, H[reg_of<D, WB, WA>(tq)], xs[c], acc);
@@ -190,18 +200,18 @@ __device__ __forceinline__ void sad4(const uint32_t* H, const uint4& x, int q, u
 }
 
 // Value of table entry e against H.
-template <int D, int WB, int WA>
+template <int D, int WB, int WA, bool LIN = false>
 __device__ __forceinline__ int entry_value(const uint32_t* H, const uint32_t* e) {
   using S = Shape<D, WB, WA>;
   const uint4* t = reinterpret_cast<const uint4*>(e);
   uint32_t a0 = 0u, a1 = 0u;
 #pragma unroll
-  for (int q = 0; q < S::NW / 4; ++q) sad4<D, WB, WA>(H, t[q], q, a0, a1);
-  return (int)(a0 + a1);
+  for (int q = 0; q < S::NW / 4; ++q) sad4<D, WB, WA, LIN>(H, t[q], q, a0, a1);
+  return (int)(a0 + a1 + (LIN ? H[0] : 0u));
 }
 
 // max over all B table entries
-template <int D, int WB, int WA>
+template <int D, int WB, int WA, bool LIN = false>
 __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, int B) {
   using S = Shape<D, WB, WA>;
   int m = INT_MIN;
@@ -214,16 +224,17 @@ __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, i
     for (int q = 0; q < S::NW / 4; ++q) {
       const uint4 x = t0[q];
       const uint4 y = t1[q];
-      sad4<D, WB, WA>(H, x, q, a0, a1);
-      sad4<D, WB, WA>(H, y, q, b0, b1);
+      sad4<D, WB, WA, LIN>(H, x, q, a0, a1);
+      sad4<D, WB, WA, LIN>(H, y, q, b0, b1);
     }
     m = max(m, max((int)(a0 + a1), (int)(b0 + b1)));
   }
-  if (j < B) m = max(m, entry_value<D, WB, WA>(H, sT + j * S::NW));
+  if (LIN && j > 0) m += (int)H[0];
+  if (j < B) m = max(m, entry_value<D, WB, WA, LIN>(H, sT + j * S::NW));
   return m;
 }
 
-template <int D, int WB, int WA>
+template <int D, int WB, int WA, bool LIN = false>
 __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs args) {
   using S = Shape<D, WB, WA>;
   constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
     for (int w = 0; w < WT; ++w) {
       if (w < WV) {
         if (D == 1) {
-          e[w] = L1[w];
+          e[w] = (LIN && w == 0) ? 0u - L1[w] : L1[w];
         } else if (D == 2) {
           e[w] = wsub<WB>(w, 0u, L1[w]);
           e[WT + w] = wsub<WB>(w, sTot[w], L1[w]);
@@ -332,7 +343,7 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
         }
         move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
       }
-      const int m = scan_max<D, WB, WA>(H, sT, B);
+      const int m = scan_max<D, WB, WA, LIN>(H, sT, B);
       if (m > best) { best = m; best_h = h0 + u; }
     }
   }
@@ -346,7 +357,7 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
     const bool rev = (best_h & 1ull) != 0ull;
     for (int jj = 0; jj < B; ++jj) {
       const int je = rev ? B - 1 - jj : jj;
-      if (entry_value<D, WB, WA>(H, sT + je * NW) == best) {
+      if (entry_value<D, WB, WA, LIN>(H, sT + je * NW) == best) {
         bn = best_h * (unsigned long long)B + (unsigned long long)jj;
         break;
       }

@@ -24,6 +24,17 @@ const void* table_kernel_mixed_ptr(int D, int WB, int WA) {
   return table_kernels()[D][WB][WA];
 }
 
+const void* table_kernel_lin_ptr(int WB, int WA) {
+  static TableKernelLinTab tab = {};
+  static bool init = [] {
+    table_register_d1_lin(tab);
+    return true;
+  }();
+  (void)init;
+  if (WB < 1 || WB > 2 || WA < 0 || WA > 16) return nullptr;
+  return tab[WB][WA];
+}
+
 const void* table_kernel_ptr(int D, int W, int PK) {
   if (PK == 1) return table_kernel_mixed_ptr(D, W, 0);
   if (PK == 4) return table_kernel_mixed_ptr(D, 0, W);
