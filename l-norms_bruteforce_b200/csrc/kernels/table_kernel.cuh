@@ -187,7 +187,10 @@ __device__ __forceinline__ void sad4(const uint32_t* H, const uint4& x, int q, u
   for (int c = 0; c < 4; ++c) {
     const int tq = 4 * q + c;
     if (computed<D, WB, WA>(tq)) {
-      uint32_t& acc = (c & 1) ? a1 : a0;
+      // short entries (up to 16 words): one dependent chain, whose latency the
+      // two entries of a scan step and the resident warps hide, with no final
+      // add; longer entries alternate two chains
+      uint32_t& acc = (S::NW > 16 && (c & 1)) ? a1 : a0;
       const int w = tq % S::WT;
       if (LIN && tq == 0)
         acc += xs[c];
