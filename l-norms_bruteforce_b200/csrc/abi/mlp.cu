@@ -30,7 +30,7 @@ cudaError_t launch_gemm(const ld::mlp::GemmArgs& g, cudaStream_t s) {
   // Each CTA holds BN of the SM's 512 TMEM columns; the shared-memory request
   // is raised so that no more CTAs share an SM than TMEM can hold at once
   // (233472 bytes of shared memory per SM, 1 KB reserved per CTA).
-  const size_t tiles = (size_t)ld::mlp::kTileM * ld::mlp::kTileK * 2 + (size_t)BN * ld::mlp::kTileK * 2;
+  const size_t tiles = 2 * ((size_t)ld::mlp::kTileM * ld::mlp::kTileK * 2 + (size_t)BN * ld::mlp::kTileK * 2);
   const size_t cap = 233472 / (512 / BN + 1) + 1024;
   const size_t smem = tiles > cap ? tiles : cap;
   cudaError_t e = cudaFuncSetAttribute(ld::mlp::tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -43,8 +43,11 @@ cudaError_t launch_gemm(const ld::mlp::GemmArgs& g, cudaStream_t s) {
 cudaError_t gemm(const bf16* A, const bf16* B, int M, int N, int K, float* C, bf16* H, bf16* HT,
                  const float* bias, int relu, int* err, cudaStream_t s) {
   ld::mlp::GemmArgs g{A, B, M, N, K, C, H, HT, bias, relu, err};
-  if (N % 256 == 0) return launch_gemm<256>(g, s);
-  if (N % 128 == 0) return launch_gemm<128>(g, s);
+  // these GEMMs are small: prefer the tile width that gives the most CTAs
+  // while a wider tile still fills the 148 SMs
+  const int tiles_m = M / ld::mlp::kTileM;
+  if (N % 256 == 0 && tiles_m * (N / 256) >= 148) return launch_gemm<256>(g, s);
+  if (N % 128 == 0 && tiles_m * (N / 128) >= 148) return launch_gemm<128>(g, s);
   return launch_gemm<64>(g, s);
 }
 

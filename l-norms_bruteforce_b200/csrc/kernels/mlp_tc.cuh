@@ -4,12 +4,12 @@
 //   C[M x N] = A[M x K] * B[N x K]^T      (A, B bf16, K-major; fp32 accumulate)
 //
 // One CTA (4 warps) computes a 128 x BN tile.  Per 64-wide K chunk the CTA
-// copies the A and B tiles into shared memory in the canonical K-major
-// layout without swizzle (8-row x 16-byte core matrices; core matrices 128 B
-// apart along K, 1024 B apart along M/N), one elected thread issues four
-// tcgen05.mma (K = 16 each) into a TMEM accumulator of 128 lanes x BN fp32
-// columns and commits them to an mbarrier, which the CTA waits on before
-// overwriting the tiles.  The epilogue reads the accumulator with
+// copies the A and B tiles (cp.async, two stages) into shared memory in the
+// canonical K-major layout without swizzle (8-row x 16-byte core matrices;
+// core matrices 128 B apart along K, 1024 B apart along M/N), one elected
+// thread issues four tcgen05.mma (K = 16 each) into a TMEM accumulator of
+// 128 lanes x BN fp32 columns and commits them to the stage's mbarrier,
+// which the CTA waits on before refilling that stage.  The epilogue reads the accumulator with
 // tcgen05.ld (warp w owns lanes 32w..32w+31, i.e. rows 32w..32w+31 of the
 // tile), optionally adds a bias and applies ReLU, and stores fp32 and/or
 // bf16 (row-major and transposed) outputs.
@@ -77,17 +77,29 @@ struct GemmArgs {
   int* err;
 };
 
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
+// Two-stage pipeline: while the tensor core multiplies chunk kc out of one
+// shared-memory stage, the CTA's threads copy chunk kc + 1 into the other
+// with cp.async.  A stage is refilled only after the mbarrier of the MMAs
+// that read it has completed.
 template <int BN>
 __global__ void __launch_bounds__(128) tc_gemm_kernel(const GemmArgs g) {
   static_assert(BN == 64 || BN == 128 || BN == 256, "tile width");
+  constexpr int kStageA = kTileM * kTileK * 2, kStageB = BN * kTileK * 2;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* sA = smem_raw;                              // 128 x 64 bf16 = 16 KB
-  unsigned char* sB = smem_raw + kTileM * kTileK * 2;        // BN x 64 bf16
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
-  __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * BN;
+  const uint32_t sbase = smem_u32(smem_raw);
+  auto sA = [&](int st) { return sbase + st * (kStageA + kStageB); };
+  auto sB = [&](int st) { return sbase + st * (kStageA + kStageB) + kStageA; };
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -95,42 +107,57 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(const GemmArgs g) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[0])), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[1])), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;");
-    s_abort = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = instr_desc(kTileM, BN);
-  uint32_t phase = 0;
-  bool ok = true;
 
-  for (int k0 = 0; k0 < g.K && ok; k0 += kTileK) {
-    // A tile: 128 rows x 8 chunks of 16 bytes
+  // chunk kc of A (128 rows) and B (BN rows) into stage st, core-matrix layout:
+  // row r, 16-byte piece c at ((r / 8) * 8 + c) * 128 + (r % 8) * 16
+  auto load = [&](int kc, int st) {
+    const int k0 = kc * kTileK;
 #pragma unroll
     for (int i = 0; i < (kTileM * 8) / 128; ++i) {
       const int q = tid + 128 * i, r = q >> 3, c = q & 7;
-      const uint4 v = *reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + r) * g.K + k0 + c * 8);
-      *reinterpret_cast<uint4*>(sA + (((r >> 3) * 8 + c) * 128) + (r & 7) * 16) = v;
+      cp_async16(sA(st) + (((r >> 3) * 8 + c) * 128) + (r & 7) * 16, g.A + (size_t)(m0 + r) * g.K + k0 + c * 8);
     }
 #pragma unroll
     for (int i = 0; i < (BN * 8) / 128; ++i) {
       const int q = tid + 128 * i, r = q >> 3, c = q & 7;
-      const uint4 v = *reinterpret_cast<const uint4*>(g.B + (size_t)(n0 + r) * g.K + k0 + c * 8);
-      *reinterpret_cast<uint4*>(sB + (((r >> 3) * 8 + c) * 128) + (r & 7) * 16) = v;
+      cp_async16(sB(st) + (((r >> 3) * 8 + c) * 128) + (r & 7) * 16, g.B + (size_t)(n0 + r) * g.K + k0 + c * 8);
+    }
+    cp_async_commit();
+  };
+
+  const int nk = g.K / kTileK;
+  bool ok = true;
+  load(0, 0);
+  for (int kc = 0; kc < nk; ++kc) {
+    const int st = kc & 1;
+    bool good = true;
+    if (kc + 1 < nk) {
+      // stage st ^ 1 was read by the MMAs of chunk kc - 1 (its ((kc-1)/2)-th use)
+      if (kc >= 1) good = mbar_wait(smem_u32(&mbar[st ^ 1]), (uint32_t)((kc - 1) >> 1) & 1u);
+      if (good) load(kc + 1, st ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     // generic-proxy shared-memory writes -> visible to the tensor core
     asm volatile("fence.proxy.async.shared::cta;");
-    __syncthreads();
+    if (__syncthreads_or(!good)) { ok = false; break; }
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
       for (int kk = 0; kk < kTileK / 16; ++kk) {
-        const uint64_t da = smem_desc(smem_u32(sA) + kk * 256, 128, 1024);
-        const uint64_t db = smem_desc(smem_u32(sB) + kk * 256, 128, 1024);
-        const uint32_t acc = (k0 > 0 || kk > 0) ? 1u : 0u;
+        const uint64_t da = smem_desc(sA(st) + kk * 256, 128, 1024);
+        const uint64_t db = smem_desc(sB(st) + kk * 256, 128, 1024);
+        const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
@@ -138,13 +165,15 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(const GemmArgs g) {
             :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   :: "r"(smem_u32(&mbar)));
+                   :: "r"(smem_u32(&mbar[st])));
     }
-    // the MMAs must have read the tiles before they are overwritten
-    if (!mbar_wait(smem_u32(&mbar), phase)) { s_abort = 1; }
-    phase ^= 1u;
-    __syncthreads();
-    if (s_abort) ok = false;
+  }
+  if (ok) {
+    // the last commit tracks every MMA issued before it
+    const bool done = mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), (uint32_t)((nk - 1) >> 1) & 1u);
+    ok = !__syncthreads_or(!done);
+  } else {
+    cp_async_wait<0>();
   }
   asm volatile("tcgen05.fence::after_thread_sync;");
 
