@@ -286,6 +286,78 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line))
 
 
+REF_GPU_BIN = ROOT / "oracle" / "_ref" / "L_CUDA"
+
+
+def run_reference_gpu(args) -> None:
+    """The reference's own CUDA solver (L_CUDA.cu built for sm_100a from its
+    sources) on the same workload file and flags, timed as its README times
+    it: wall clock of the whole process.  Its launch shape (blocks x
+    threads, CLI arguments) is swept and the fastest kept.  The process's
+    fixed cost (CUDA context, parsing) is measured on a 2 x 2 matrix and
+    reported, and subtracted in `value_minus_startup`."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if args.config == 4 or args.method != "plain":
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "the reference solves one matrix per "
+                          "process by plain enumeration"}))
+        return
+    if not REF_GPU_BIN.exists():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/L_CUDA was not built "
+                          "(make -C oracle needs the reference sources)"}))
+        return
+    ld = load_package()
+    inst = instance(args.config)
+    info = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal).info
+    tail = inst.argv_tail()
+
+    def run(a, blocks, threads, tail_args):
+        with tempfile.TemporaryDirectory() as td:
+            write_matrix(Path(td) / "m.txt", a)
+            t0 = time.perf_counter()
+            p = subprocess.run([str(REF_GPU_BIN), str(blocks), str(threads), "m.txt", *tail_args], cwd=td,
+                               capture_output=True, text=True, timeout=600)
+            dt = time.perf_counter() - t0
+        if p.returncode != 0:
+            raise RuntimeError(f"reference GPU solver failed: {p.stdout[-300:]} {p.stderr[-300:]}")
+        return dt, p.stdout
+
+    startup = min(run(np.array([[1, 2], [3, 4]]), 1, 1, ["1"])[0] for _ in range(3))
+    shapes = [(512, 32), (148 * 8, 128), (148 * 16, 128), (148 * 32, 256), (148 * 64, 256)]
+    if args.ref_launch:
+        shapes = [tuple(int(x) for x in args.ref_launch.split("x"))]
+    sweep = {}
+    for b, t in shapes:
+        dt, out = run(inst.matrix, b, t, tail)
+        sweep[f"{b}x{t}"] = dt
+        if dt > 120:
+            break
+    best = min(sweep, key=sweep.get)
+    b, t = (int(x) for x in best.split("x"))
+    for _ in range(args.warmup):
+        run(inst.matrix, b, t, tail)
+    times, out = [], ""
+    for _ in range(args.steps):
+        dt, out = run(inst.matrix, b, t, tail)
+        times.append(dt)
+    value_line = next((ln for ln in out.splitlines() if " is: " in ln), "")
+    wall = statistics.mean(times)
+    n = int(info["labelings"])
+    line = {
+        "impl": "reference-gpu", "metric": "exact L_d labelings/s (plain enumeration)", "value": n / wall,
+        "unit": "labelings/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded generator of the configuration)",
+        "config": {"workload": workload_name(inst, info), "launch": best, "sweep_s": sweep,
+                   "output": value_line.strip()},
+        "value_minus_startup": n / max(wall - startup, 1e-6), "startup_s": startup,
+        "note": "L_CUDA.cu compiled from the reference sources for sm_100a (oracle/_ref/L_CUDA); whole-process "
+                "wall clock, as the reference's README measures it",
+    }
+    print(json.dumps(line))
+
+
 def workload_name(inst, info) -> str:
     return (f"{inst.name}: d={info['d_user']}{' marginal' if info['marginal_user'] else ''}, "
             f"flag {inst.stat}, {info['rows_in']}x{info['cols_in']} -> {info['rows']}x{info['cols']}, "
@@ -615,17 +687,21 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
                     help="workload; 4 runs the batched solver over the 4096-matrix batch")
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--method", default="plain", choices=["plain", "pruned", "learned"],
                     help="plain enumeration (the headline), or the exact pruned search with an "
                          "incumbent from random (pruned) or network (learned) proposals")
     ap.add_argument("--proposals", type=int, default=8, help="proposals per solve (pruned / learned)")
+    ap.add_argument("--ref-launch", default="",
+                    help="reference-gpu: blocks x threads to use (e.g. 9472x256) instead of the sweep")
     ap.add_argument("--with-plain", action="store_true",
                     help="also time one plain enumeration of the workload (pruned / learned)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.impl == "reference-gpu":
+        run_reference_gpu(args)
     elif args.config == 4:
         run_batch(args)
     elif args.method != "plain":
