@@ -13,6 +13,8 @@
 
 #include <climits>
 #include <cstdint>
+#include <cstring>
+#include <mutex>
 
 #include "../host/ld_internal.h"
 
@@ -111,11 +113,22 @@ __global__ void __launch_bounds__(kLsWarps * 32) local_search_kernel(const LsArg
 #define LS_CUDA(call)                                                                \
   do {                                                                               \
     cudaError_t e_ = (call);                                                         \
-    if (e_ != cudaSuccess) {                                                         \
-      st = ld_fail(LD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));            \
-      goto done;                                                                     \
-    }                                                                                \
+    if (e_ != cudaSuccess) return ld_fail(LD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
+
+// Per-device workspace kept between calls: one device arena, one pinned
+// staging buffer (inputs out, results back in one copy each) and a stream.
+struct LsWorkspace {
+  char* dmem = nullptr;
+  size_t dcap = 0;
+  char* hmem = nullptr;
+  size_t hcap = 0;
+  cudaStream_t stream = nullptr;
+};
+std::mutex g_ls_mu[64];
+LsWorkspace g_ls[64];
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 
@@ -126,25 +139,39 @@ extern "C" ld_status ld_local_search(const int64_t* a, int32_t R, int32_t C, int
     return ld_fail(LD_ERR_ARG, "bad local-search arguments");
   if (d < 1 || d > 3 || C > kLsMaxCols || R > kLsMaxRows)
     return ld_fail(LD_ERR_LIMIT, "local search takes d <= 3, <= %d columns, <= %d rows", kLsMaxCols, kLsMaxRows);
+  if (device < 0 || device >= 64) return ld_fail(LD_ERR_ARG, "device %d out of range", device);
   for (int64_t t = 0; t < (int64_t)n * (R - 1); ++t)
     if (starts[t] < 0 || starts[t] >= (d == 1 ? 2 : d)) return ld_fail(LD_ERR_ARG, "start label out of range");
-  ld_status st = LD_OK;
-  long long* dA = nullptr; int* dStarts = nullptr; long long* dVal = nullptr; int* dLab = nullptr;
-  LsArgs args;
   const size_t nl = (size_t)n * (R - 1);
+  // inputs: matrix | starts; results: values | labels
+  const size_t bA = up256(sizeof(long long) * (size_t)R * C), bS = up256(sizeof(int) * nl);
+  const size_t bV = up256(sizeof(long long) * (size_t)n), bL = up256(sizeof(int) * nl);
+  const size_t in_bytes = bA + bS, out_bytes = bV + bL, total = in_bytes + out_bytes;
   if (cudaSetDevice(device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "no device %d", device);
-  LS_CUDA(cudaMalloc(&dA, sizeof(long long) * (size_t)R * C));
-  LS_CUDA(cudaMalloc(&dStarts, sizeof(int) * nl));
-  LS_CUDA(cudaMalloc(&dVal, sizeof(long long) * n));
-  LS_CUDA(cudaMalloc(&dLab, sizeof(int) * nl));
-  LS_CUDA(cudaMemcpy(dA, a, sizeof(long long) * (size_t)R * C, cudaMemcpyHostToDevice));
-  LS_CUDA(cudaMemcpy(dStarts, starts, sizeof(int) * nl, cudaMemcpyHostToDevice));
-  args = LsArgs{dA, R, C, d, marginal, dStarts, n, max_rounds > 0 ? max_rounds : 4 * R, dVal, dLab};
-  local_search_kernel<<<(n + kLsWarps - 1) / kLsWarps, kLsWarps * 32>>>(args);
+  std::lock_guard<std::mutex> lock(g_ls_mu[device]);
+  LsWorkspace& w = g_ls[device];
+  if (!w.stream) LS_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+  if (w.dcap < total) {
+    if (w.dmem) { LS_CUDA(cudaStreamSynchronize(w.stream)); LS_CUDA(cudaFree(w.dmem)); w.dmem = nullptr; w.dcap = 0; }
+    LS_CUDA(cudaMalloc(&w.dmem, total));
+    w.dcap = total;
+  }
+  if (w.hcap < total) {
+    if (w.hmem) { LS_CUDA(cudaStreamSynchronize(w.stream)); LS_CUDA(cudaFreeHost(w.hmem)); w.hmem = nullptr; w.hcap = 0; }
+    LS_CUDA(cudaMallocHost(&w.hmem, total));
+    w.hcap = total;
+  }
+  memcpy(w.hmem, a, sizeof(long long) * (size_t)R * C);
+  memcpy(w.hmem + bA, starts, sizeof(int) * nl);
+  LS_CUDA(cudaMemcpyAsync(w.dmem, w.hmem, in_bytes, cudaMemcpyHostToDevice, w.stream));
+  LsArgs args{(const long long*)w.dmem, R, C, d, marginal, (const int*)(w.dmem + bA), n,
+              max_rounds > 0 ? max_rounds : 4 * R, (long long*)(w.dmem + in_bytes),
+              (int*)(w.dmem + in_bytes + bV)};
+  local_search_kernel<<<(n + kLsWarps - 1) / kLsWarps, kLsWarps * 32, 0, w.stream>>>(args);
   LS_CUDA(cudaGetLastError());
-  LS_CUDA(cudaMemcpy(values, dVal, sizeof(long long) * n, cudaMemcpyDeviceToHost));
-  LS_CUDA(cudaMemcpy(labels, dLab, sizeof(int) * nl, cudaMemcpyDeviceToHost));
-done:
-  cudaFree(dA); cudaFree(dStarts); cudaFree(dVal); cudaFree(dLab);
-  return st;
+  LS_CUDA(cudaMemcpyAsync(w.hmem + in_bytes, w.dmem + in_bytes, out_bytes, cudaMemcpyDeviceToHost, w.stream));
+  LS_CUDA(cudaStreamSynchronize(w.stream));
+  memcpy(values, w.hmem + in_bytes, sizeof(long long) * (size_t)n);
+  memcpy(labels, w.hmem + in_bytes + bV, sizeof(int) * nl);
+  return LD_OK;
 }
