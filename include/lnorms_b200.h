@@ -18,8 +18,8 @@
  *  - A plan is single-threaded and runs on one CUDA stream (its own, or the
  *    one given in ld_options).
  *  - Matrix entries are int64 on the host.  The device path computes in
- *    packed int8x4 / int16x2, int32 or int64 lanes, chosen from an exact
- *    bound on every partial column sum, so results never overflow.
+ *    packed int8x4, int32 or int64 lanes, chosen from an exact bound on
+ *    every partial column sum, so results never overflow.
  */
 #ifndef LNORMS_B200_H
 #define LNORMS_B200_H
@@ -76,7 +76,9 @@ typedef struct {
     int32_t lane_bits;          /* 0 auto, else force 16 / 32 / 64 (>= needed)    */
     int32_t shard_index;        /* this device's part of a solve split over       */
     int32_t shard_count;        /* shard_count devices (0 or 1: the whole range)  */
-    int32_t reserved;
+    int32_t prune_policy;       /* ld_solve_pruned: 0 = run the plain enumeration
+                                   instead when more than a quarter of the walk
+                                   prefixes survive their bound; 1 = always scan */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

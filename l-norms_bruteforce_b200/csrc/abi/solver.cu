@@ -831,6 +831,19 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     if ((e = cudaLaunchKernel(kb, dim3((unsigned)blocks_b), dim3(ld::kPruneThreads), params, smem_b, s)) != cudaSuccess)
       return fail("walk bound launch", e);
     if ((e = cudaEventRecord(r->ev1, s)) != cudaSuccess) return fail("event", e);
+    // When more than a quarter of the walks survive their bound the scan
+    // would do most of the plain enumeration's work at a lower rate: run the
+    // plain enumeration instead (same result).
+    if ((e = cudaMemcpyAsync(hstat, dmem + off_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) !=
+        cudaSuccess)
+      return fail("survivors", e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail("walk bound", e);
+    if (o.prune_policy == 0 && hstat[0] * 4ull > walks) {
+      cudaEventElapsedTime(&ms_b, r->ev0, r->ev1);
+      ps.walks_kept = hstat[0];
+      ps.bound_ms = ms_b;
+      return plain();
+    }
     if ((e = cudaLaunchKernel(ks, dim3((unsigned)blocks_s), dim3(ld::kPruneThreads), params, smem_s, s)) != cudaSuccess)
       return fail("scan launch", e);
     if ((e = cudaEventRecord(r->ev2, s)) != cudaSuccess) return fail("event", e);

@@ -234,10 +234,27 @@ def test_pruned_equals_plain(ld, case):
     best = labs[int(np.argmax(vals))]
     opt = O.labels(ref[1], a.shape[0], d)
     for inc in (None, best, opt, labs[int(np.argmin(vals))]):
-        sol, st = ld.solve_pruned(a, d, marg, inc)
-        assert (sol.value, sol.gray_index) == ref, st
-        if inc is not None:
-            assert st["incumbent"] == O.value(a, d, marg, inc)
+        for policy in (0, 1):           # automatic fallback, and always scan the survivors
+            sol, st = ld.solve_pruned(a, d, marg, inc, ld.options(prune_policy=policy))
+            assert (sol.value, sol.gray_index) == ref, st
+            if inc is not None:
+                assert st["incumbent"] == O.value(a, d, marg, inc)
+            if policy == 1 and st["walk_rows"] > 0:
+                assert st["pruned"] == 1
+
+
+def test_pruned_falls_back_to_plain_when_bounds_prune_little(ld):
+    """Random N(0, 20^2) matrices with d = 3 keep most walk prefixes: the
+    automatic policy runs the plain enumeration, with the same answer."""
+    rng = np.random.default_rng(7)
+    a = np.rint(rng.normal(0, 20, size=(16, 24))).astype(np.int64)
+    ref = O.enumerate_max(a, 3, False)
+    vals, labs = ld.local_search(a, 3, False, n_random=64, seed=1)
+    sol, st = ld.solve_pruned(a, 3, False, labs[int(np.argmax(vals))])
+    assert (sol.value, sol.gray_index) == ref
+    assert st["pruned"] == 0 and st["walks_kept"] * 4 > st["walks_total"]
+    sol, st = ld.solve_pruned(a, 3, False, labs[int(np.argmax(vals))], ld.options(prune_policy=1))
+    assert (sol.value, sol.gray_index) == ref and st["pruned"] == 1
 
 
 def test_pruned_skips_most_blocks_on_low_rank(ld, workloads):
