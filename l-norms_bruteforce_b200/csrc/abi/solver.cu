@@ -1187,8 +1187,8 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   };
 
   // autotuner: walks per thread per chunk and the persistent grid size, timed
-  // on each class's leading chunks (its largest matrices); cached per class
-  // shape and matrix size.
+  // on one wave of each class's chunks from its median matrix on; cached per
+  // class shape and matrix size.
   for (auto& c : b->classes) {
     double mean = 0;
     for (int p : c.probs) mean += (double)walks[p];
@@ -1205,9 +1205,18 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     double best_frac = 1.0;
     for (int wpt : {1, 2, 4, 8}) {
       for (double frac : {1.0}) {
-        std::vector<ld::BatchChunk> chunks;
-        batch_chunks(b, c, wpt, walks, &chunks);
-        const int sample = std::min<int>((int)chunks.size(), 2 * di.sms * c.bps);
+        std::vector<ld::BatchChunk> all;
+        batch_chunks(b, c, wpt, walks, &all);
+        // one wave of chunks (a chunk per resident CTA), starting at the
+        // class's median matrix: the class's steady state at a fraction of
+        // the cost of its largest matrices
+        const int wave = di.sms * c.bps;
+        size_t first = 0;
+        const int median = c.probs[c.probs.size() / 2];
+        while (first < all.size() && all[first].problem != median) ++first;
+        if (first + (size_t)wave > all.size()) first = all.size() > (size_t)wave ? all.size() - wave : 0;
+        std::vector<ld::BatchChunk> chunks(all.begin() + first, all.end());
+        const int sample = std::min<int>((int)chunks.size(), wave);
         if (sample < 1) continue;
         cudaMemcpy(b->dmem + b->off_chunks, chunks.data(), sizeof(ld::BatchChunk) * sample, cudaMemcpyHostToDevice);
         BatchClass tc = c;
