@@ -209,6 +209,40 @@ def test_config2_uses_mixed_lanes(ld, workloads):
     plan.close()
 
 
+@pytest.mark.parametrize("seed", range(16))
+def test_lm_linear_column(ld, seed):
+    """LM with the marginal column in a 32-bit word of its own runs the
+    instances that add it linearly; value and Gray index match the oracle
+    for one or two 32-bit words and 0..16 int8x4 words, including ties."""
+    rng = np.random.default_rng(500 + seed)
+    r = int(rng.integers(6, 21))
+    c = int(rng.integers(1, 66)) if seed % 4 else int(rng.integers(1, 5))
+    a = rng.integers(-2, 3, size=(r, c)).astype(np.int64)
+    a[:, 0] = rng.integers(-60, 61, size=r)                 # forces a 32-bit marginal column
+    if seed % 3 == 0 and c > 2:
+        a[:, 1] = rng.integers(-90, 91, size=r)             # and a second 32-bit column
+    if seed % 5 == 0:
+        a[1] = a[0]                                         # tied rows
+    ref = O.enumerate_max(a, 1, True)
+    plan = ld.Plan(a, 1, True)
+    desc = plan.describe()
+    if "int32 words=1 " in desc or "int32 words=2 " in desc:
+        assert "lin=1" in desc, desc
+    sol = plan.solve()
+    assert (sol.value, sol.gray_index) == ref, desc
+    plan.close()
+
+
+def test_lm_linear_column_is_chosen(ld):
+    rng = np.random.default_rng(9)
+    a = rng.integers(-2, 3, size=(14, 23)).astype(np.int64)
+    a[:, 0] = rng.integers(-60, 61, size=14)
+    plan = ld.Plan(a, 1, True)
+    assert "int32 words=1 " in plan.describe() and "lin=1" in plan.describe()
+    assert (plan.solve().value, plan.solve().gray_index) == O.enumerate_max(a, 1, True)
+    plan.close()
+
+
 def prune_cases():
     rng = np.random.default_rng(77)
     for t in range(18):
