@@ -1204,7 +1204,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     int best_wpt = 1;
     double best_frac = 1.0;
     for (int wpt : {1, 2, 4, 8}) {
-      for (double frac : {1.0}) {
+      for (double frac : {0.5, 1.0}) {   // persistent CTAs: half or all of the occupancy limit
         std::vector<ld::BatchChunk> all;
         batch_chunks(b, c, wpt, walks, &all);
         // one wave of chunks (a chunk per resident CTA), starting at the
