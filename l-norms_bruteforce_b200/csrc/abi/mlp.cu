@@ -26,17 +26,33 @@ constexpr int kIn = 44, kInP = 64, kHid = 256, kOut = 44, kOutP = 64, kOutGP = 1
   } while (0)
 
 template <int BN>
-cudaError_t launch_gemm(const ld::mlp::GemmArgs& g, cudaStream_t s) {
+size_t gemm_smem() {
   // Each CTA holds BN of the SM's 512 TMEM columns; the shared-memory request
   // is raised so that no more CTAs share an SM than TMEM can hold at once
   // (233472 bytes of shared memory per SM, 1 KB reserved per CTA).
   const size_t tiles = 2 * ((size_t)ld::mlp::kTileM * ld::mlp::kTileK * 2 + (size_t)BN * ld::mlp::kTileK * 2);
   const size_t cap = 233472 / (512 / BN + 1) + 1024;
-  const size_t smem = tiles > cap ? tiles : cap;
-  cudaError_t e = cudaFuncSetAttribute(ld::mlp::tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  return tiles > cap ? tiles : cap;
+}
+
+// Shared-memory limits of the three GEMM instances; called before any
+// launch on the current device (and before any stream capture).
+cudaError_t gemm_init() {
+  cudaError_t e = cudaFuncSetAttribute(ld::mlp::tc_gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)gemm_smem<64>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ld::mlp::tc_gemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gemm_smem<128>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ld::mlp::tc_gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gemm_smem<256>());
+  return e;
+}
+
+template <int BN>
+cudaError_t launch_gemm(const ld::mlp::GemmArgs& g, cudaStream_t s) {
   dim3 grid(g.M / ld::mlp::kTileM, g.N / BN);
-  ld::mlp::tc_gemm_kernel<BN><<<grid, 128, smem, s>>>(g);
+  ld::mlp::tc_gemm_kernel<BN><<<grid, 128, gemm_smem<BN>(), s>>>(g);
   return cudaGetLastError();
 }
 
@@ -67,9 +83,16 @@ struct ld_mlp {
   // bf16 operands
   bf16 *W1b, *W2b, *W2T, *W3b, *W3T;
   bf16 *Xb, *XT, *H1, *H1T, *H2, *H2T, *dZ3, *dZ3T, *dZ2, *dZ2T, *dZ1T;
-  float *Xf, *Z3, *Tt, *Mk, *dH2, *dH1, *loss;
+  float *Xf, *Z3, *Tt, *Mk, *dH2, *dH1, *loss, *hp;
   int* err;
   int step = 0;
+  // pinned staging: inputs (x, targets, mask, step parameters) and results
+  // (logits, loss, error flag); the graphs copy from and to these
+  void* hmem = nullptr;
+  float *hX, *hT, *hM, *hHp, *hZ, *hLoss;
+  int* hErr;
+  // captured CUDA graphs: one training step, one forward pass
+  cudaGraphExec_t train_exec = nullptr, fwd_exec = nullptr;
 };
 
 namespace {
@@ -103,67 +126,120 @@ cudaError_t refresh_bf16(ld_mlp* n) {
   return cudaGetLastError();
 }
 
-ld_status upload_batch(ld_mlp* n, const float* x, const float* t, const float* mask, int rows) {
-  std::vector<float> X((size_t)n->batch * kInP, 0.f), T, M;
-  for (int r = 0; r < rows; ++r) memcpy(&X[(size_t)r * kInP], x + (size_t)r * kIn, sizeof(float) * kIn);
-  MLP_CUDA(cudaMemcpyAsync(n->Xf, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, n->s));
-  if (t) {
-    T.assign((size_t)n->batch * kOutP, 0.f);
-    M.assign((size_t)n->batch * kOutP, 0.f);
-    for (int r = 0; r < rows; ++r)
-      for (int c = 0; c < kOut; ++c) {
-        T[(size_t)r * kOutP + c] = t[(size_t)r * kOut + c];
-        M[(size_t)r * kOutP + c] = mask[(size_t)r * kOut + c];
-      }
-    MLP_CUDA(cudaMemcpyAsync(n->Tt, T.data(), sizeof(float) * T.size(), cudaMemcpyHostToDevice, n->s));
-    MLP_CUDA(cudaMemcpyAsync(n->Mk, M.data(), sizeof(float) * M.size(), cudaMemcpyHostToDevice, n->s));
-  }
+// Host staging of one batch: rows of x (44 features) and, for training, of
+// targets and mask, zero-padded to the device layout (batch x 64).  Returns
+// 1 / (number of unmasked targets), or 0 when there are none.
+float stage_batch(ld_mlp* n, const float* x, const float* t, const float* mask, int rows) {
+  memset(n->hX, 0, sizeof(float) * (size_t)n->batch * kInP);
+  for (int r = 0; r < rows; ++r) memcpy(n->hX + (size_t)r * kInP, x + (size_t)r * kIn, sizeof(float) * kIn);
+  if (!t) return 0.f;
+  memset(n->hT, 0, sizeof(float) * (size_t)n->batch * kOutP);
+  memset(n->hM, 0, sizeof(float) * (size_t)n->batch * kOutP);
+  double cnt = 0;
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < kOut; ++c) {
+      n->hT[(size_t)r * kOutP + c] = t[(size_t)r * kOut + c];
+      n->hM[(size_t)r * kOutP + c] = mask[(size_t)r * kOut + c];
+      cnt += mask[(size_t)r * kOut + c];
+    }
+  return cnt > 0 ? (float)(1.0 / cnt) : 0.f;
+}
+
+// the staged inputs to the device, x to bf16 (and transposed)
+cudaError_t enqueue_upload(ld_mlp* n, bool targets) {
+  const size_t bx = sizeof(float) * (size_t)n->batch * kInP, bt = sizeof(float) * (size_t)n->batch * kOutP;
+  cudaError_t e = cudaMemcpyAsync(n->Xf, n->hX, bx, cudaMemcpyHostToDevice, n->s);
+  if (e == cudaSuccess && targets) e = cudaMemcpyAsync(n->Tt, n->hT, bt, cudaMemcpyHostToDevice, n->s);
+  if (e == cudaSuccess && targets) e = cudaMemcpyAsync(n->Mk, n->hM, bt, cudaMemcpyHostToDevice, n->s);
+  if (e == cudaSuccess && targets)
+    e = cudaMemcpyAsync(n->hp, n->hHp, sizeof(float) * ld::mlp::kHpWords, cudaMemcpyHostToDevice, n->s);
+  if (e != cudaSuccess) return e;
   ld::mlp::to_bf16_kernel<<<blocks_for(n->batch * kInP), 256, 0, n->s>>>(n->Xf, n->batch, kInP, n->Xb, n->XT);
-  MLP_CUDA(cudaGetLastError());
-  return LD_OK;
+  return cudaGetLastError();
 }
 
-ld_status forward(ld_mlp* n) {
+cudaError_t enqueue_forward(ld_mlp* n) {
   const int B = n->batch;
-  MLP_CUDA(gemm(n->Xb, n->W1b, B, kHid, kInP, nullptr, n->H1, n->H1T, n->b1, 1, n->err, n->s));
-  MLP_CUDA(gemm(n->H1, n->W2b, B, kHid, kHid, nullptr, n->H2, n->H2T, n->b2, 1, n->err, n->s));
-  MLP_CUDA(gemm(n->H2, n->W3b, B, kOutP, kHid, n->Z3, nullptr, nullptr, n->b3, 0, n->err, n->s));
-  return LD_OK;
+  cudaError_t e = gemm(n->Xb, n->W1b, B, kHid, kInP, nullptr, n->H1, n->H1T, n->b1, 1, n->err, n->s);
+  if (e == cudaSuccess) e = gemm(n->H1, n->W2b, B, kHid, kHid, nullptr, n->H2, n->H2T, n->b2, 1, n->err, n->s);
+  if (e == cudaSuccess) e = gemm(n->H2, n->W3b, B, kOutP, kHid, n->Z3, nullptr, nullptr, n->b3, 0, n->err, n->s);
+  return e;
 }
 
-ld_status backward(ld_mlp* n, float inv_count) {
+cudaError_t enqueue_backward(ld_mlp* n) {
   const int B = n->batch;
-  MLP_CUDA(cudaMemsetAsync(n->loss, 0, sizeof(float), n->s));
+  cudaError_t e = cudaMemsetAsync(n->loss, 0, sizeof(float), n->s);
+  if (e != cudaSuccess) return e;
   // Xf and Z3 share the padded 64-column layout, so the residual input of
   // output column c is input column c
   static_assert(kInP == kOutP, "residual path needs equal padded widths");
-  ld::mlp::bce_grad_kernel<<<blocks_for(B * kOutP), 256, 0, n->s>>>(n->Z3, n->Tt, n->Mk, B, kOutP, inv_count,
+  ld::mlp::bce_grad_kernel<<<blocks_for(B * kOutP), 256, 0, n->s>>>(n->Z3, n->Tt, n->Mk, B, kOutP, n->hp,
                                                                      n->skip != 0.f ? n->Xf : nullptr, n->skip,
                                                                      n->dZ3, n->dZ3T, n->loss);
-  MLP_CUDA(cudaGetLastError());
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // W3: [kOutGP x B] x [kHid x B]^T (rows kOutP.. of dZ3T are zero)
-  MLP_CUDA(gemm(n->dZ3T, n->H2T, kOutGP, kHid, B, n->gW3, nullptr, nullptr, nullptr, 0, n->err, n->s));
-  MLP_CUDA(gemm(n->dZ3, n->W3T, B, kHid, kOutP, n->dH2, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  if ((e = gemm(n->dZ3T, n->H2T, kOutGP, kHid, B, n->gW3, nullptr, nullptr, nullptr, 0, n->err, n->s)) != cudaSuccess) return e;
+  if ((e = gemm(n->dZ3, n->W3T, B, kHid, kOutP, n->dH2, nullptr, nullptr, nullptr, 0, n->err, n->s)) != cudaSuccess) return e;
   ld::mlp::relu_grad_kernel<<<blocks_for(B * kHid), 256, 0, n->s>>>(n->dH2, n->H2, B, kHid, n->dZ2, n->dZ2T);
-  MLP_CUDA(cudaGetLastError());
-  MLP_CUDA(gemm(n->dZ2T, n->H1T, kHid, kHid, B, n->gW2, nullptr, nullptr, nullptr, 0, n->err, n->s));
-  MLP_CUDA(gemm(n->dZ2, n->W2T, B, kHid, kHid, n->dH1, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = gemm(n->dZ2T, n->H1T, kHid, kHid, B, n->gW2, nullptr, nullptr, nullptr, 0, n->err, n->s)) != cudaSuccess) return e;
+  if ((e = gemm(n->dZ2, n->W2T, B, kHid, kHid, n->dH1, nullptr, nullptr, nullptr, 0, n->err, n->s)) != cudaSuccess) return e;
   ld::mlp::relu_grad_kernel<<<blocks_for(B * kHid), 256, 0, n->s>>>(n->dH1, n->H1, B, kHid, nullptr, n->dZ1T);
-  MLP_CUDA(cudaGetLastError());
-  MLP_CUDA(gemm(n->dZ1T, n->XT, kHid, kInP, B, n->gW1, nullptr, nullptr, nullptr, 0, n->err, n->s));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = gemm(n->dZ1T, n->XT, kHid, kInP, B, n->gW1, nullptr, nullptr, nullptr, 0, n->err, n->s)) != cudaSuccess) return e;
   ld::mlp::bias_grad_kernel<<<kHid / 4, 128, 0, n->s>>>(n->dZ1T, kHid, B, n->gb1);
   ld::mlp::bias_grad_kernel<<<kHid / 4, 128, 0, n->s>>>(n->dZ2T, kHid, B, n->gb2);
   ld::mlp::bias_grad_kernel<<<kOutP / 4, 128, 0, n->s>>>(n->dZ3T, kOutP, B, n->gb3);
-  MLP_CUDA(cudaGetLastError());
+  return cudaGetLastError();
+}
+
+cudaError_t enqueue_adam(ld_mlp* n) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  for (int i = 0; i < 6; ++i) {
+    const PShape& sh = kShapes[i];
+    bf16* wb = i == 0 ? n->W1b : i == 2 ? n->W2b : i == 4 ? n->W3b : nullptr;
+    bf16* wbT = i == 2 ? n->W2T : i == 4 ? n->W3T : nullptr;
+    ld::mlp::adam_kernel<<<blocks_for(sh.rows * sh.cols), 256, 0, n->s>>>(
+        *params_of(n, i), *grads_of(n, i), n->m[i], n->v[i], sh.rows, sh.cols, n->hp, b1, b2, eps, wb, wbT);
+  }
+  return cudaGetLastError();
+}
+
+// loss and error flag (and, for a forward pass, the logits) back to staging
+cudaError_t enqueue_results(ld_mlp* n, bool logits) {
+  cudaError_t e = cudaMemcpyAsync(n->hLoss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, n->s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(n->hErr, n->err, sizeof(int), cudaMemcpyDeviceToHost, n->s);
+  if (e == cudaSuccess && logits)
+    e = cudaMemcpyAsync(n->hZ, n->Z3, sizeof(float) * (size_t)n->batch * kOutP, cudaMemcpyDeviceToHost, n->s);
+  return e;
+}
+
+// Capture `body` on the network's stream into an executable graph.
+template <typename F>
+ld_status capture(ld_mlp* n, F body, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  MLP_CUDA(cudaStreamBeginCapture(n->s, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t e = body();
+  const cudaError_t e2 = cudaStreamEndCapture(n->s, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return ld_fail(LD_ERR_CUDA, "network graph capture failed: %s",
+                   cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  const cudaError_t e3 = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) return ld_fail(LD_ERR_CUDA, "network graph: %s", cudaGetErrorString(e3));
   return LD_OK;
 }
 
-ld_status check_err(ld_mlp* n) {
-  int e = 0;
-  MLP_CUDA(cudaMemcpyAsync(&e, n->err, sizeof e, cudaMemcpyDeviceToHost, n->s));
+// wait for the stream; report (and clear) a GEMM whose bounded wait ran out
+ld_status finish(ld_mlp* n) {
   MLP_CUDA(cudaStreamSynchronize(n->s));
-  if (e) {
+  if (*n->hErr) {
+    const int e = *n->hErr;
+    *n->hErr = 0;
     cudaMemsetAsync(n->err, 0, sizeof(int), n->s);
+    cudaStreamSynchronize(n->s);
     return ld_fail(LD_ERR_TIMEOUT, "tensor-core GEMM wait ran out (code %d)", e);
   }
   return LD_OK;
@@ -201,6 +277,7 @@ extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int
   f32(&n->Xf, (size_t)B * kInP); f32(&n->Z3, (size_t)B * kOutP); f32(&n->Tt, (size_t)B * kOutP);
   f32(&n->Mk, (size_t)B * kOutP); f32(&n->dH2, (size_t)B * kHid); f32(&n->dH1, (size_t)B * kHid);
   f32(&n->loss, 1);
+  f32(&n->hp, ld::mlp::kHpWords);
   pieces.push_back({(void**)&n->err, 4});
   size_t total = 0;
   for (auto& pc : pieces) total += (pc.bytes + 255) & ~(size_t)255;
@@ -223,9 +300,40 @@ extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int
       for (int c = 0; c < sh.hcols; ++c) w[(size_t)r * sh.cols + c] = U(rng);
     cudaMemcpy(*params_of(n, i), w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
   }
-  if (refresh_bf16(n) != cudaSuccess || cudaStreamSynchronize(n->s) != cudaSuccess) {
+  if (refresh_bf16(n) != cudaSuccess || cudaStreamSynchronize(n->s) != cudaSuccess || gemm_init() != cudaSuccess) {
     ld_mlp_destroy(n);
     return ld_fail(LD_ERR_CUDA, "network initialisation failed");
+  }
+  // pinned staging: x, targets, mask (batch x 64 each), logits (batch x 64),
+  // step parameters, loss, error flag
+  const size_t slab = sizeof(float) * (size_t)B * 64;
+  if (cudaMallocHost(&n->hmem, 4 * slab + 256) != cudaSuccess) {
+    ld_mlp_destroy(n);
+    return ld_fail(LD_ERR_CUDA, "pinned staging allocation failed");
+  }
+  char* h = (char*)n->hmem;
+  n->hX = (float*)h; n->hT = (float*)(h + slab); n->hM = (float*)(h + 2 * slab); n->hZ = (float*)(h + 3 * slab);
+  n->hHp = (float*)(h + 4 * slab); n->hLoss = (float*)(h + 4 * slab + 64); n->hErr = (int*)(h + 4 * slab + 128);
+  memset(n->hmem, 0, 4 * slab + 256);
+  // one training step and one forward pass as CUDA graphs over fixed buffers
+  ld_status st = capture(n, [&] {
+    cudaError_t e = enqueue_upload(n, true);
+    if (e == cudaSuccess) e = enqueue_forward(n);
+    if (e == cudaSuccess) e = enqueue_backward(n);
+    if (e == cudaSuccess) e = enqueue_adam(n);
+    if (e == cudaSuccess) e = enqueue_results(n, false);
+    return e;
+  }, &n->train_exec);
+  if (st == LD_OK)
+    st = capture(n, [&] {
+      cudaError_t e = enqueue_upload(n, false);
+      if (e == cudaSuccess) e = enqueue_forward(n);
+      if (e == cudaSuccess) e = enqueue_results(n, true);
+      return e;
+    }, &n->fwd_exec);
+  if (st != LD_OK) {
+    ld_mlp_destroy(n);
+    return st;
   }
   *out = n;
   return LD_OK;
@@ -234,8 +342,12 @@ extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int
 extern "C" void ld_mlp_destroy(ld_mlp* n) {
   if (!n) return;
   cudaSetDevice(n->device);
-  if (n->s) { cudaStreamSynchronize(n->s); cudaStreamDestroy(n->s); }
+  if (n->s) cudaStreamSynchronize(n->s);
+  if (n->train_exec) cudaGraphExecDestroy(n->train_exec);
+  if (n->fwd_exec) cudaGraphExecDestroy(n->fwd_exec);
+  if (n->s) cudaStreamDestroy(n->s);
   if (n->mem) cudaFree(n->mem);
+  if (n->hmem) cudaFreeHost(n->hmem);
   delete n;
 }
 
@@ -275,18 +387,15 @@ extern "C" ld_status ld_mlp_set_params(ld_mlp* n, const float* params) {
 extern "C" ld_status ld_mlp_forward(ld_mlp* n, const float* x, int32_t rows, float* logits) {
   if (!n || !x || !logits || rows < 1) return ld_fail(LD_ERR_ARG, "bad arguments");
   MLP_CUDA(cudaSetDevice(n->device));
-  std::vector<float> z((size_t)n->batch * kOutP);
   for (int r0 = 0; r0 < rows; r0 += n->batch) {
     const int cnt = std::min(n->batch, rows - r0);
-    ld_status st = upload_batch(n, x + (size_t)r0 * kIn, nullptr, nullptr, cnt);
-    if (st == LD_OK) st = forward(n);
-    if (st != LD_OK) return st;
-    MLP_CUDA(cudaMemcpyAsync(z.data(), n->Z3, sizeof(float) * z.size(), cudaMemcpyDeviceToHost, n->s));
-    st = check_err(n);
+    stage_batch(n, x + (size_t)r0 * kIn, nullptr, nullptr, cnt);
+    MLP_CUDA(cudaGraphLaunch(n->fwd_exec, n->s));
+    ld_status st = finish(n);
     if (st != LD_OK) return st;
     for (int r = 0; r < cnt; ++r)
       for (int c = 0; c < kOut; ++c)
-        logits[(size_t)(r0 + r) * kOut + c] = z[(size_t)r * kOutP + c] + n->skip * x[(size_t)(r0 + r) * kIn + c];
+        logits[(size_t)(r0 + r) * kOut + c] = n->hZ[(size_t)r * kOutP + c] + n->skip * x[(size_t)(r0 + r) * kIn + c];
   }
   return LD_OK;
 }
@@ -296,15 +405,14 @@ extern "C" ld_status ld_mlp_gradients(ld_mlp* n, const float* x, const float* t,
                                       float* grads, float* loss) {
   if (!n || !x || !t || !mask || rows < 1 || rows > n->batch) return ld_fail(LD_ERR_ARG, "bad arguments");
   MLP_CUDA(cudaSetDevice(n->device));
-  double cnt = 0;
-  for (size_t i = 0; i < (size_t)rows * kOut; ++i) cnt += mask[i];
-  ld_status st = upload_batch(n, x, t, mask, rows);
-  if (st == LD_OK) st = forward(n);
-  if (st == LD_OK) st = backward(n, cnt > 0 ? (float)(1.0 / cnt) : 0.f);
+  n->hHp[ld::mlp::kHpInvCount] = stage_batch(n, x, t, mask, rows);
+  MLP_CUDA(enqueue_upload(n, true));
+  MLP_CUDA(enqueue_forward(n));
+  MLP_CUDA(enqueue_backward(n));
+  MLP_CUDA(enqueue_results(n, false));
+  ld_status st = finish(n);
   if (st != LD_OK) return st;
-  st = check_err(n);
-  if (st != LD_OK) return st;
-  if (loss) MLP_CUDA(cudaMemcpy(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) *loss = *n->hLoss;
   if (grads) {
     float* dst = grads;
     for (int i = 0; i < 6; ++i) {
@@ -319,22 +427,20 @@ extern "C" ld_status ld_mlp_gradients(ld_mlp* n, const float* x, const float* t,
   return LD_OK;
 }
 
+// One Adam step: a single launch of the captured training graph.
 extern "C" ld_status ld_mlp_train_step(ld_mlp* n, const float* x, const float* t, const float* mask, int32_t rows,
                                        float lr, float* loss) {
-  ld_status st = ld_mlp_gradients(n, x, t, mask, rows, nullptr, loss);
-  if (st != LD_OK) return st;
+  if (!n || !x || !t || !mask || rows < 1 || rows > n->batch) return ld_fail(LD_ERR_ARG, "bad arguments");
+  MLP_CUDA(cudaSetDevice(n->device));
   n->step += 1;
-  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-  const float c1 = 1.f - std::pow(b1, (float)n->step), c2 = 1.f - std::pow(b2, (float)n->step);
-  for (int i = 0; i < 6; ++i) {
-    const PShape& sh = kShapes[i];
-    bf16* wb = i == 0 ? n->W1b : i == 2 ? n->W2b : i == 4 ? n->W3b : nullptr;
-    bf16* wbT = i == 2 ? n->W2T : i == 4 ? n->W3T : nullptr;
-    ld::mlp::adam_kernel<<<blocks_for(sh.rows * sh.cols), 256, 0, n->s>>>(
-        *params_of(n, i), *grads_of(n, i), n->m[i], n->v[i], sh.rows, sh.cols, lr, b1, b2, eps, c1, c2, wb, wbT);
-  }
-  MLP_CUDA(cudaGetLastError());
-  MLP_CUDA(cudaStreamSynchronize(n->s));
+  n->hHp[ld::mlp::kHpInvCount] = stage_batch(n, x, t, mask, rows);
+  n->hHp[ld::mlp::kHpLr] = lr;
+  n->hHp[ld::mlp::kHpC1] = 1.f - std::pow(0.9f, (float)n->step);
+  n->hHp[ld::mlp::kHpC2] = 1.f - std::pow(0.999f, (float)n->step);
+  MLP_CUDA(cudaGraphLaunch(n->train_exec, n->s));
+  ld_status st = finish(n);
+  if (st != LD_OK) return st;
+  if (loss) *loss = *n->hLoss;
   return LD_OK;
 }
 
@@ -345,6 +451,7 @@ extern "C" ld_status ld_tc_gemm(const uint16_t* A, const uint16_t* B, int32_t M,
   if (!A || !B || !C || M < 128 || M % 128 || N < 64 || N % 64 || K < 64 || K % 64)
     return ld_fail(LD_ERR_ARG, "shape must be M%%128, N%%64, K%%64");
   MLP_CUDA(cudaSetDevice(device));
+  MLP_CUDA(gemm_init());
   void* mem = nullptr;
   const size_t ba = (size_t)M * K * 2, bb = (size_t)N * K * 2, bc = (size_t)M * N * 4;
   MLP_CUDA(cudaMalloc(&mem, ba + bb + bc + 256));

@@ -226,14 +226,20 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(const GemmArgs g) {
 
 // ---- element-wise parts ---------------------------------------------------
 
+// Step parameters read from device memory, so that one captured CUDA graph
+// serves every training step: learning rate, Adam bias corrections
+// 1 - beta1^t and 1 - beta2^t, and 1 / (number of unmasked targets).
+enum { kHpLr = 0, kHpC1 = 1, kHpC2 = 2, kHpInvCount = 3, kHpWords = 4 };
+
 // BCE with logits over valid entries: dz = (sigmoid(z) - t) * mask / count,
 // written as bf16 (row-major and transposed); loss accumulated.  The logit
 // is the network output plus `skip` times the input of the same index
 // (a residual path without parameters; skip_x may be null).
 __global__ void bce_grad_kernel(const float* z, const float* t, const float* mask, int rows, int cols,
-                                float inv_count, const float* skip_x, float skip, __nv_bfloat16* dz,
+                                const float* hp, const float* skip_x, float skip, __nv_bfloat16* dz,
                                 __nv_bfloat16* dzT, float* loss) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const float inv_count = hp[kHpInvCount];
   float l = 0.f;
   if (i < rows * cols) {
     const int r = i / cols, c = i % cols;
@@ -272,12 +278,13 @@ __global__ void bias_grad_kernel(const __nv_bfloat16* dzT, int cols, int rows, f
 }
 
 // Adam on fp32 master weights w (rows x cols, gradient g); refreshes the
-// bf16 copy wb and its transpose wbT (either may be null).
-__global__ void adam_kernel(float* w, const float* g, float* m, float* v, int rows, int cols, float lr,
-                            float b1, float b2, float eps, float c1, float c2, __nv_bfloat16* wb,
-                            __nv_bfloat16* wbT) {
+// bf16 copy wb and its transpose wbT (either may be null).  Learning rate
+// and bias corrections come from the step parameters hp.
+__global__ void adam_kernel(float* w, const float* g, float* m, float* v, int rows, int cols, const float* hp,
+                            float b1, float b2, float eps, __nv_bfloat16* wb, __nv_bfloat16* wbT) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= rows * cols) return;
+  const float lr = hp[kHpLr], c1 = hp[kHpC1], c2 = hp[kHpC2];
   const float gi = g[i];
   const float mi = b1 * m[i] + (1.f - b1) * gi;
   const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
