@@ -531,7 +531,7 @@ def run_batch(args) -> None:
     ld = load_package()
     import lnorms_b200.workloads as W
     mats, ds, skipped, skipped_lab, total, slots = [], [], 0, 0, 0, 0
-    for inst in W.config4():
+    for inst in W.config4()[: args.batch_count or None]:
         p = ld.Problem.from_matrix(inst.matrix, inst.d)
         info = p.info
         if info["d"] == 3 and info["labelings"] > 3 ** 20:
@@ -580,7 +580,7 @@ def run_batch(args) -> None:
         "unit": "labelings/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator of the configuration)",
-        "config": {"workload": f"config4: {len(mats)} of 4096 matrices, {total} labelings",
+        "config": {"workload": f"config4: {len(mats)} of {args.batch_count or 4096} matrices, {total} labelings",
                    "matrices": len(mats), "labelings_per_step": total,
                    "skipped": {"matrices": skipped, "labelings": skipped_lab,
                                "why": "d = 3 with more than 3^20 labelings"},
@@ -693,6 +693,8 @@ def main() -> None:
                     help="plain enumeration (the headline), or the exact pruned search with an "
                          "incumbent from random (pruned) or network (learned) proposals")
     ap.add_argument("--proposals", type=int, default=8, help="proposals per solve (pruned / learned)")
+    ap.add_argument("--batch-count", type=int, default=0,
+                    help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")
     ap.add_argument("--ref-launch", default="",
                     help="reference-gpu: blocks x threads to use (e.g. 9472x256) instead of the sweep")
     ap.add_argument("--with-plain", action="store_true",
