@@ -55,10 +55,12 @@ def _pkg():
 # ---- features ---------------------------------------------------------------
 
 def spectral_basis(a: np.ndarray, k: int = 3) -> np.ndarray:
-    """Top-k right singular vectors (m x k) of a (rows x cols) matrix."""
+    """Top-k right singular vectors (m x k) of a (rows x cols) matrix: the
+    eigenvectors of A^T A with the k largest eigenvalues (signs arbitrary;
+    a direction and its negation give the same labeling)."""
     a = np.asarray(a, dtype=np.float64)
-    _, _, vt = np.linalg.svd(a, full_matrices=False)
-    v = vt[:k].T
+    _, u = np.linalg.eigh(a.T @ a)
+    v = u[:, ::-1][:, :k]
     if v.shape[1] < k:
         v = np.concatenate([v, np.zeros((v.shape[0], k - v.shape[1]))], axis=1)
     return v
