@@ -263,6 +263,9 @@ void ld_batch_destroy(ld_batch *b);
 /* of x are 44 features, rows of t / mask 44 targets in [0,1] and weights   */
 /* (0 drops an entry).  Parameters travel as one flat fp32 array: W1[256x44] */
 /* b1[256] W2[256x256] b2[256] W3[44x256] b3[44] (ld_mlp_param_count()).    */
+/* A network object owns its device buffers, pinned staging, stream and two
+ * captured CUDA graphs (a training step, a forward pass); use it from one
+ * thread at a time. */
 typedef struct ld_mlp ld_mlp;
 /* batch: rows per device pass, a positive multiple of 128.  skip: weight of
  * a parameter-free residual path, logits = W3 h2 + b3 + skip * x (the
