@@ -42,6 +42,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "smem_limit.h"
 #include "../host/ld_internal.h"
 #include "../kernels/common.cuh"
 #include "../kernels/registry.h"
@@ -150,7 +151,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   while (k < F && ipow(base, k + 1) <= (unsigned long long)maxB) ++k;
   const int B = (int)ipow(base, k);
   const size_t smem = (size_t)ld::table_smem_words(d, W, R, B) * sizeof(uint32_t);
-  e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  e = ld_raise_smem_limit(kfn, smem);
   if (e != cudaSuccess) return ld_fail(LD_ERR_CUDA, "shared memory attribute: %s", cudaGetErrorString(e));
   int bps = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kfn, ld::kTableThreads, smem);

@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "smem_limit.h"
 #include "../host/ld_internal.h"
 #include "../kernels/common.cuh"
 #include "../kernels/registry.h"
@@ -112,6 +113,7 @@ bool table_config(const int64_t* a, int R, int C, int d, int marginal, int k, in
     narrow.clear();
     WB = C; WA = 0;
   }
+  if (d >= 4 && WA == 0) WB = round4(WB);      // d >= 4: 32-bit instances come in multiples of 4 words
   if (!ld::table_kernel_mixed_ptr(d, WB, WA)) {
     if (force_bits == 8 || C > 64 || !ld::table_kernel_mixed_ptr(d, C, 0)) return false;
     wide.clear();
@@ -138,7 +140,7 @@ ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, con
   const bool fits32 = vmax <= (long long)INT32_MAX && maxabs <= (long long)INT32_MAX;
   if (o.lane_bits && o.lane_bits != 8 && o.lane_bits != 32 && o.lane_bits != 64)
     return ld_fail(LD_ERR_ARG, "lane width %d is not 8, 32 or 64", o.lane_bits);
-  if (o.kernel != LD_KERNEL_WIDE && d <= 3 && o.lane_bits != 64 && fits32) {
+  if (o.kernel != LD_KERNEL_WIDE && d <= 10 && o.lane_bits != 64 && fits32) {
     const int base = d <= 2 ? 2 : d, F = R - 1;
     double best_t = 0;
     bool found = false;
@@ -385,7 +387,7 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     p->B = (int)ipow(base, k);
     p->tpb = ld::kTableThreads;
     p->smem = (size_t)ld::table_smem_words(D, WT, R, p->B) * sizeof(uint32_t);
-    if (cudaFuncSetAttribute(p->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem) != cudaSuccess) {
+    if (ld_raise_smem_limit(p->kfn, p->smem) != cudaSuccess) {
       delete p; return ld_fail(LD_ERR_CUDA, "cannot reserve %zu bytes of shared memory", p->smem);
     }
     int bps = 0;
@@ -772,8 +774,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
   const size_t smem_s = (size_t)ld::prune_smem_words(d, WT, R, B, true) * 4;
   int bps_b = 0, bps_s = 0;
   if (cudaSetDevice(o.device) != cudaSuccess ||
-      cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b) != cudaSuccess ||
-      cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s) != cudaSuccess ||
+      ld_raise_smem_limit(kb, smem_b) != cudaSuccess || ld_raise_smem_limit(ks, smem_s) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, kb, ld::kPruneThreads, smem_b) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_s, ks, ld::kPruneThreads, smem_s) != cudaSuccess ||
       bps_b < 1 || bps_s < 1)
@@ -1107,7 +1108,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   for (auto& c : b->classes) {
     std::stable_sort(c.probs.begin(), c.probs.end(),
                      [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
-    if (cudaFuncSetAttribute(c.kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem) != cudaSuccess ||
+    if (ld_raise_smem_limit(c.kfn, c.smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps, c.kfn, ld::kBatchThreads, c.smem) != cudaSuccess ||
         c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {

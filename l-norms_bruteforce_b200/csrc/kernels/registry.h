@@ -3,18 +3,20 @@
 
 namespace ld {
 
-// table_kernel<D, WB, WA> by (D, WB, WA): D in 1..3, WB int32 words (0..64),
+// table_kernel<D, WB, WA> by (D, WB, WA): D in 1..10, WB int32 words (0..64),
 // WA int8x4 words (0..32).  Instances:
 //   D = 1: WB <= 4 with WA <= 16 (mixed), WA <= 32 with WB = 0, WB <= 64 with WA = 0
 //   D = 2: WB <= 64 with WA = 0, WA <= 32 with WB = 0
 //   D = 3: WB <= 64 with WA = 0, WA <= 32 with WB = 0
-using TableKernelTab = const void* [4][65][33];
+//   D = 4..10: WA in 1..8 with WB = 0, WB in 4, 8, 12, 16 with WA = 0
+using TableKernelTab = const void* [11][65][33];
 void table_register_d1_mix(TableKernelTab& t);
 void table_register_d1_p8(TableKernelTab& t);
 void table_register_d1_p32a(TableKernelTab& t);
 void table_register_d1_p32b(TableKernelTab& t);
 void table_register_d2(TableKernelTab& t);
 void table_register_d3(TableKernelTab& t);
+void table_register_dn(TableKernelTab& t);
 
 // table_kernel<1, WB, WA, true> (LM, marginal column linear in word 0) by
 // (WB, WA): WB in 1..2, WA in 0..16

@@ -79,8 +79,9 @@ struct Shape {
   static constexpr int WV = WB + WA;                  // computed words per vector
   static constexpr int WT = (WV + 3) & ~3;            // padded words per vector
   static constexpr int NW = D * WT;                   // words per table entry
-  // register vectors: D = 3 keeps H1, H2 and (up to 32 words) H1 + H2
-  static constexpr int NR = D == 3 ? (WV > 32 ? 2 : 3) : 1;
+  // register vectors: D = 3 keeps H1, H2 and (up to 32 words) H1 + H2;
+  // D >= 4 keeps H_1 .. H_{D-1} and their sum
+  static constexpr int NR = D == 3 ? (WV > 32 ? 2 : 3) : (D >= 4 ? D : 1);
 };
 
 template <int WB>
@@ -118,6 +119,16 @@ __device__ __forceinline__ void move_row(uint32_t* H, const uint32_t* row, int a
     else   { sub_row<D, WB, WA>(H, row, 0); sub_row<D, WB, WA>(H, row, 0); }
   } else if (D == 2) {
     if (b) add_row<D, WB, WA>(H, row, 0); else sub_row<D, WB, WA>(H, row, 0);
+  } else if (D >= 4) {
+    // vector v holds the rows labelled v + 1; vector D - 1 their sum (the
+    // unrolled tests keep every register index a compile-time constant)
+#pragma unroll
+    for (int v = 0; v < D - 1; ++v) {
+      if (a == v + 1) sub_row<D, WB, WA>(H, row, v);
+      if (b == v + 1) add_row<D, WB, WA>(H, row, v);
+    }
+    if (a == 0 && b != 0) add_row<D, WB, WA>(H, row, D - 1);
+    if (a != 0 && b == 0) sub_row<D, WB, WA>(H, row, D - 1);
   } else {
     if (a == 1) sub_row<D, WB, WA>(H, row, 0);
     if (a == 2) sub_row<D, WB, WA>(H, row, 1);
@@ -149,6 +160,19 @@ __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const
       if (D == 1) { if (lab) add_row<D, WB, WA>(H, row, 0); else sub_row<D, WB, WA>(H, row, 0); }
       else if (lab) add_row<D, WB, WA>(H, row, 0);
     }
+  } else if (D >= 4) {
+    unsigned long long q = h;
+    for (int t = 0; t < nh; ++t) {
+      const int r = (int)(q % (2ull * D));
+      const int lab = r < D ? r : 2 * D - 1 - r;
+      q /= (unsigned long long)D;
+      if (lab == 0) continue;
+      const uint32_t* row = sA + (k + t) * S::WT;
+#pragma unroll
+      for (int v = 0; v < D - 1; ++v)
+        if (lab == v + 1) add_row<D, WB, WA>(H, row, v);
+      add_row<D, WB, WA>(H, row, D - 1);
+    }
   } else {
     unsigned long long q = h;
     for (int t = 0; t < nh; ++t) {
@@ -162,11 +186,35 @@ __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const
   }
 }
 
+// Table entry (low labeling) whose labels equal the low rows' labels at
+// Gray index N = h * B + j, for D >= 4.  The low rows' labels are the
+// reflected code's digits 0..k-1 of N; entry e was tabulated with the
+// labels of e's own digits, so e is the inverse of that code applied to
+// these labels (top digit first: a digit's label is mirrored when the
+// number formed by the digits above it is odd).
+template <int D>
+__device__ __forceinline__ int low_entry(unsigned long long N, int k) {
+  int lab[16];
+  unsigned long long q = N;
+  for (int t = 0; t < k; ++t) {
+    const int r = (int)(q % (2ull * D));
+    lab[t] = r < D ? r : 2 * D - 1 - r;
+    q /= (unsigned long long)D;
+  }
+  int e = 0, p = 0;
+  for (int t = k - 1; t >= 0; --t) {
+    const int digit = p ? D - 1 - lab[t] : lab[t];
+    e = e * D + digit;
+    p = (D % 2 == 0) ? (digit & 1) : ((p + digit) & 1);
+  }
+  return e;
+}
+
 // register word compared with table word q (q in [0, NW))
 template <int D, int WB, int WA>
 __device__ __forceinline__ constexpr int reg_of(int q) {
   using S = Shape<D, WB, WA>;
-  return (D == 3 ? (q / S::WT) : 0) * S::WV + q % S::WT;
+  return (D >= 3 ? (q / S::WT) : 0) * S::WV + q % S::WT;
 }
 template <int D, int WB, int WA>
 __device__ __forceinline__ constexpr bool computed(int q) {
@@ -237,6 +285,51 @@ __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, i
   return m;
 }
 
+// D >= 4: tabulate, for every low labeling j (reflected base-D Gray word of
+// j), the vectors -L_1 .. -L_{D-1} (L_m: the low rows labelled m) and
+// T - (L_1 + .. + L_{D-1}).
+template <int D, int WB, int WA>
+__device__ __forceinline__ void build_table_dn(const uint32_t* sA, const uint32_t* sTot, uint32_t* sT, int k, int B) {
+  using S = Shape<D, WB, WA>;
+  constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
+  for (int j = threadIdx.x; j < B; j += blockDim.x) {
+    uint32_t L[D - 1][WV];
+#pragma unroll
+    for (int v = 0; v < D - 1; ++v)
+#pragma unroll
+      for (int w = 0; w < WV; ++w) L[v][w] = 0u;
+    unsigned q = (unsigned)j;
+    for (int i = 0; i < k; ++i) {
+      const unsigned r = q % (2u * D);
+      const int lab = r < (unsigned)D ? (int)r : 2 * D - 1 - (int)r;
+      q /= (unsigned)D;
+      const uint32_t* row = sA + i * WT;
+#pragma unroll
+      for (int v = 0; v < D - 1; ++v)
+        if (lab == v + 1) {
+#pragma unroll
+          for (int w = 0; w < WV; ++w) L[v][w] = wadd<WB>(w, L[v][w], row[w]);
+        }
+    }
+    uint32_t* e = sT + j * NW;
+#pragma unroll
+    for (int w = 0; w < WT; ++w) {
+      if (w < WV) {
+        uint32_t rest = sTot[w];
+#pragma unroll
+        for (int v = 0; v < D - 1; ++v) {
+          e[v * WT + w] = wsub<WB>(w, 0u, L[v][w]);
+          rest = wsub<WB>(w, rest, L[v][w]);
+        }
+        e[(D - 1) * WT + w] = rest;
+      } else {
+#pragma unroll
+        for (int v = 0; v < D; ++v) e[v * WT + w] = 0u;
+      }
+    }
+  }
+}
+
 template <int D, int WB, int WA, bool LIN = false>
 __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs args) {
   using S = Shape<D, WB, WA>;
@@ -259,6 +352,8 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
   __syncthreads();
 
   // Tabulate the low rows' partial sums for every low labeling j (Gray order).
+  if constexpr (D >= 4) build_table_dn<D, WB, WA>(sA, sTot, sT, k, B);
+  else
   for (int j = threadIdx.x; j < B; j += blockDim.x) {
     uint32_t L1[WV], L2[WV];
 #pragma unroll
@@ -334,6 +429,18 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
           i = __ffsll((long long)u) - 1;            // == ctz(h): h0 is a multiple of 2^fw
           b = (int)(((h >> (i + 1)) & 1ull) ^ 1ull);
           a = b ^ 1;
+        } else if (D >= 4) {
+          // digit i (the lowest nonzero base-D digit of u) steps from c - 1
+          // to c; its label is mirrored when h / D^(i+1) is odd
+          unsigned long long q = u;
+          i = 0;
+          while (q % (unsigned long long)D == 0ull) { q /= (unsigned long long)D; ++i; }
+          const int c = (int)(q % (unsigned long long)D);
+          unsigned long long hh = h;
+          for (int t = 0; t <= i; ++t) hh /= (unsigned long long)D;
+          const int par = (int)(hh & 1ull);
+          b = par ? D - 1 - c : c;
+          a = par ? D - c : c - 1;
         } else {
           unsigned long long q = u;
           i = 0;
@@ -359,7 +466,10 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
     seed_high<D, WB, WA>(H, sA, sH0, k, nh, best_h);
     const bool rev = (best_h & 1ull) != 0ull;
     for (int jj = 0; jj < B; ++jj) {
-      const int je = rev ? B - 1 - jj : jj;
+      // d <= 3: the low word is read backwards for odd h; D >= 4: the entry
+      // is found from the labels (for even D only the top low digit mirrors)
+      const int je = D >= 4 ? low_entry<(D >= 4 ? D : 4)>(best_h * (unsigned long long)B + (unsigned long long)jj, k)
+                            : (rev ? B - 1 - jj : jj);
       if (entry_value<D, WB, WA, LIN>(H, sT + je * NW) == best) {
         bn = best_h * (unsigned long long)B + (unsigned long long)jj;
         break;

@@ -13,6 +13,7 @@ static const TableKernelTab& table_kernels() {
     table_register_d1_p32b(tab);
     table_register_d2(tab);
     table_register_d3(tab);
+    table_register_dn(tab);
     return true;
   }();
   (void)init;
@@ -20,7 +21,7 @@ static const TableKernelTab& table_kernels() {
 }
 
 const void* table_kernel_mixed_ptr(int D, int WB, int WA) {
-  if (D < 1 || D > 3 || WB < 0 || WB > 64 || WA < 0 || WA > 32) return nullptr;
+  if (D < 1 || D > 10 || WB < 0 || WB > 64 || WA < 0 || WA > 32) return nullptr;
   return table_kernels()[D][WB][WA];
 }
 

@@ -233,6 +233,54 @@ def test_lm_linear_column(ld, seed):
     plan.close()
 
 
+@pytest.mark.parametrize("d", [4, 5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("lanes", ["int8", "int32"])
+def test_table_kernel_d4_to_d10(ld, d, lanes):
+    """The table decomposition for L_4 .. L_10: value and smallest Gray
+    index equal the oracle's and the wide kernel's, for 8-bit and 32-bit
+    lanes (widths padded to a multiple of 4 words), with tied rows."""
+    rng = np.random.default_rng(1000 * d + (lanes == "int32"))
+    for t in range(3):
+        r = {4: 9, 5: 8, 6: 7, 7: 7, 8: 6, 9: 6, 10: 6}[d] + t % 2
+        if lanes == "int8":
+            c = int(rng.integers(2, 33))
+            a = rng.integers(-3, 4, size=(r, c)).astype(np.int64)
+        else:
+            c = int(rng.integers(2, 17))
+            a = rng.integers(-40, 41, size=(r, c)).astype(np.int64)
+        if t == 2:
+            a[1] = a[0]
+        ref = O.enumerate_max(a, d, False)
+        plan = ld.Plan(a, d, False)
+        desc = plan.describe()
+        assert desc.startswith("table"), desc
+        sol = plan.solve()
+        plan.close()
+        assert (sol.value, sol.gray_index) == ref, desc
+        wide = ld.solve_reduced(a, d, False, ld.options(kernel=2))
+        assert (wide.value, wide.gray_index) == ref
+
+
+def test_plans_sharing_a_kernel_keep_their_shared_memory(ld):
+    """Two plans on the same kernel instance: the one created second needs
+    less dynamic shared memory; the first still launches (the per-function
+    limit is only ever raised)."""
+    rng = np.random.default_rng(31)
+    big = rng.integers(-3, 4, size=(22, 24)).astype(np.int64)
+    small = rng.integers(-3, 4, size=(8, 24)).astype(np.int64)
+    pa = ld.Plan(big, 1)
+    pb = ld.Plan(small, 1)
+    da, db = pa.describe(), pb.describe()
+    assert da.split(" k=")[0] == db.split(" k=")[0]               # same instance
+    assert int(da.split("smem=")[1]) > int(db.split("smem=")[1])
+    sa = pa.solve()
+    assert (sa.value, sa.gray_index) == O.enumerate_max(big, 1, False)
+    sb = pb.solve()
+    assert (sb.value, sb.gray_index) == O.enumerate_max(small, 1, False)
+    pa.close()
+    pb.close()
+
+
 def test_lm_linear_column_is_chosen(ld):
     rng = np.random.default_rng(9)
     a = rng.integers(-2, 3, size=(14, 23)).astype(np.int64)

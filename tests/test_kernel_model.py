@@ -68,3 +68,75 @@ def test_table_decomposition_matches_oracle(seed):
     a = rng.integers(-4, 5, size=(R, C)).astype(np.int64)
     k = int(rng.integers(0, R))       # 0 .. F low rows
     assert table_model(a, d, marginal, k) == O.enumerate_max(a, d, marginal, nthreads=1)
+
+
+# ---- d >= 4: the generic base-D step and the low-entry inverse ------------
+
+def reflected_labels(N, ndig, d):
+    """Labels of digits 0..ndig-1 of N in the reflected base-d code."""
+    out = []
+    for _ in range(ndig):
+        r = N % (2 * d)
+        out.append(r if r < d else 2 * d - 1 - r)
+        N //= d
+    return out
+
+
+def low_entry(N, k, d):
+    """The kernel's low_entry: the isolated low word whose labels equal the
+    low digits' labels of N (table_kernel.cuh)."""
+    lab = reflected_labels(N, k, d)
+    e, p = 0, 0
+    for t in range(k - 1, -1, -1):
+        digit = d - 1 - lab[t] if p else lab[t]
+        e = e * d + digit
+        p = (digit & 1) if d % 2 == 0 else ((p + digit) & 1)
+    return e
+
+
+@pytest.mark.parametrize("d", [4, 5, 6, 7, 8, 9, 10])
+def test_reflected_code_matches_oracle(d):
+    rows = 6
+    for N in range(0, d ** (rows - 1), max(1, d ** (rows - 1) // 97)):
+        assert reflected_labels(N, rows - 1, d) == list(O.labels(N, rows, d))
+
+
+@pytest.mark.parametrize("d", [4, 5, 6, 8, 10])
+@pytest.mark.parametrize("k", [0, 1, 2, 3])
+def test_low_entry_inverts_the_low_labels(d, k):
+    B = d ** k
+    for h in range(0, 7):
+        seen = set()
+        for jj in range(B):
+            N = h * B + jj
+            e = low_entry(N, k, d)
+            assert 0 <= e < B
+            assert reflected_labels(e, k, d) == reflected_labels(N, k, d)
+            seen.add(e)
+        assert len(seen) == B                        # a bijection for every h
+
+
+@pytest.mark.parametrize("d", [4, 5, 6, 9, 10])
+def test_generic_step_moves_one_row(d):
+    """The kernel's step for D >= 4: walking h within a walk, digit i (the
+    lowest nonzero base-d digit of u) moves from label a to label b with
+    par = (h / d^(i+1)) odd."""
+    ndig, fw = 5, 3
+    WL = d ** fw
+    for wk in (0, 1, 2, 5):
+        h0 = wk * WL
+        prev = reflected_labels(h0, ndig, d)
+        for u in range(1, WL):
+            h = h0 + u
+            q, i = u, 0
+            while q % d == 0:
+                q //= d
+                i += 1
+            c = q % d
+            par = (h // d ** (i + 1)) & 1
+            b = d - 1 - c if par else c
+            a = d - c if par else c - 1
+            cur = reflected_labels(h, ndig, d)
+            changed = [t for t in range(ndig) if cur[t] != prev[t]]
+            assert changed == [i] and prev[i] == a and cur[i] == b, (h, i, a, b)
+            prev = cur
