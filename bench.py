@@ -601,6 +601,44 @@ def run_batch(args) -> None:
     print(json.dumps(line))
 
 
+def run_search_batch(args, ld, L, inst, info, proposer, local, world, rank) -> None:
+    """`--count N`: N independent matrices of the workload's distribution
+    (seeds 5 .. 5 + N - 1 of the generator) solved exactly per step, the
+    network's proposals for all of them from one forward pass."""
+    import lnorms_b200.workloads as W
+    mats = [W.config5(seed=5 + i).matrix for i in range(args.count)]
+    for _ in range(args.warmup):
+        ref = L.solve_learned_batch(mats, proposer)
+    clocks = ClockSampler(local)
+    walls = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = L.solve_learned_batch(mats, proposer)
+        walls.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    proposer.close()
+    for (s0, _), (s1, _) in zip(ref, res):
+        assert (s0.value, s0.gray_index) == (s1.value, s1.gray_index)
+    if rank != 0:
+        return
+    wall = sum(walls)
+    total = info["labelings"] * args.count
+    line = {
+        "metric": f"exact L_1 labelings/s ({args.method} search, batched)", "value": total * args.steps / wall,
+        "unit": "labelings/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator of the configuration)",
+        "config": {"workload": f"{args.count} matrices of {inst.name}'s distribution (seeds 5..{4 + args.count})",
+                   "labelings_per_step": total, "proposals_per_matrix": proposer.count(),
+                   "ms_per_matrix": 1e3 * wall / args.steps / args.count,
+                   "values": [r[0].value for r in res][:8]},
+        "e2e": {"value": total * args.steps / wall, "unit": "labelings/s"},
+        "roofline": None,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def run_search(args) -> None:
     """Exact solve by the pruned enumeration with an incumbent from
     local-search-polished proposals: `--method learned` (the trained
@@ -624,6 +662,9 @@ def run_search(args) -> None:
         raise SystemExit("the learned search handles L_1 without marginals")
     mode = "network" if args.method == "learned" else "random"
     proposer = L.Proposer(mode, directions=args.proposals, samples=1, device=local)
+    if args.count > 1:
+        run_search_batch(args, ld, L, inst, info, proposer, local, world, rank)
+        return
     for _ in range(args.warmup):
         sol0, _ = L.solve_learned(red, proposer)
     torch.cuda.synchronize()
@@ -693,6 +734,8 @@ def main() -> None:
                     help="plain enumeration (the headline), or the exact pruned search with an "
                          "incumbent from random (pruned) or network (learned) proposals")
     ap.add_argument("--proposals", type=int, default=8, help="proposals per solve (pruned / learned)")
+    ap.add_argument("--count", type=int, default=1,
+                    help="pruned / learned: solve this many matrices of the workload's distribution per step")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")
     ap.add_argument("--ref-launch", default="",

@@ -305,3 +305,36 @@ def evaluate(mats, optimum, proposer: Proposer) -> dict:
     return {"mode": proposer.mode, "proposals": proposer.count(), "matrices": len(gaps),
             "optimal_rate": hits / k, "mean_gap": float(np.mean(gaps)) if gaps else 0.0,
             "raw_best_ratio": float(np.mean(raw)) if raw else 0.0, "seconds": secs}
+
+
+def solve_learned_batch(mats, proposer: Proposer, opts=None):
+    """Exact L_1 solves of many reduced matrices (each <= 44 rows): the
+    proposals of every matrix come from one forward pass of the network
+    over all their directions; then per matrix the polished incumbent and
+    the pruned enumeration.  Returns [(Solution, stats)] in input order; each
+    Solution equals the plain enumeration's."""
+    ld = _pkg()
+    mats = [np.ascontiguousarray(np.asarray(a, dtype=np.int64)) for a in mats]
+    if proposer.mode != "network":
+        return [solve_learned(a, proposer, opts) for a in mats]
+    t0 = time.perf_counter()
+    dirs = hemisphere(proposer.directions)
+    feats = [row_features(a, spectral_basis(a), dirs) for a in mats]
+    z = proposer.net.forward(np.concatenate(feats, axis=0))
+    t1 = time.perf_counter()
+    out = []
+    for p, a in enumerate(mats):
+        n = a.shape[0]
+        zp = z[p * len(dirs):(p + 1) * len(dirs), :n]
+        s = np.where(zp >= 0, 1, -1)
+        t2 = time.perf_counter()
+        values, labels = ld.local_search(a, 1, False, starts=labels_from_signs(s), device=proposer.device)
+        best = int(np.argmax(values))
+        t3 = time.perf_counter()
+        sol, pst = ld.solve_pruned(a, 1, False, labels[best], opts)
+        t4 = time.perf_counter()
+        st = {"incumbent": int(values[best]), "raw_best": int(l1_value(a, s).max()),
+              "propose_s": (t1 - t0) / len(mats), "local_search_s": t3 - t2, "pruned_s": t4 - t3}
+        st.update({f"prune_{k}": v for k, v in pst.items()})
+        out.append((sol, st))
+    return out

@@ -97,3 +97,34 @@ def test_network_gain_on_lowrank_44(ld, L, workloads, trained):
     for mode, (sol, _) in out.items():
         assert (sol.value, sol.gray_index) == (ref.value, ref.gray_index) == (7023, 7492441473292)
     assert out["network"][1]["raw_best"] > out["random"][1]["raw_best"]
+
+
+@pytest.mark.parametrize("rows", [26, 30])
+def test_lowrank_44_subblocks_match_oracle(ld, L, workloads, trained, rows):
+    """CPU parity on the 44 x 44 low-rank workload's leading row blocks (all
+    44 columns): the plain enumeration, the pruned search and the learned
+    search give the oracle's value and Gray index."""
+    import oracle_ffi as O
+    a = np.ascontiguousarray(workloads.config5().matrix[:rows])
+    ref = O.enumerate_max(a, 1, False)
+    plain = ld.solve_reduced(a, 1)
+    assert (plain.value, plain.gray_index) == ref
+    p = L.Proposer("network", directions=8, params=trained)
+    sol, st = L.solve_learned(a, p)
+    p.close()
+    assert (sol.value, sol.gray_index) == ref
+    vals, labs = ld.local_search(a, 1, False, n_random=8, seed=2)
+    sol, _ = ld.solve_pruned(a, 1, False, labs[int(np.argmax(vals))], ld.options(prune_policy=1))
+    assert (sol.value, sol.gray_index) == ref
+
+
+def test_learned_batch_equals_plain(ld, L, workloads, trained):
+    rng = np.random.default_rng(23)
+    mats = [workloads.lowrank(int(n), 44, rng) for n in rng.integers(10, 27, size=12)]
+    p = L.Proposer("network", directions=8, params=trained)
+    res = L.solve_learned_batch(mats, p)
+    p.close()
+    for a, (sol, st) in zip(mats, res):
+        plain = ld.solve_reduced(a, 1)
+        assert (sol.value, sol.gray_index) == (plain.value, plain.gray_index)
+        assert st["incumbent"] <= plain.value
