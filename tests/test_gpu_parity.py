@@ -259,6 +259,14 @@ def test_table_kernel_d4_to_d10(ld, d, lanes):
         assert (sol.value, sol.gray_index) == ref, desc
         wide = ld.solve_reduced(a, d, False, ld.options(kernel=2))
         assert (wide.value, wide.gray_index) == ref
+        # walks of several high indices (the base-d step) and every low-row count
+        for opts in (dict(tile=1), dict(tile=3), dict(low_rows=0, tile=2), dict(low_rows=1, tile=2),
+                     dict(low_rows=2, tile=1)):
+            plan = ld.Plan(a, d, False, ld.options(kernel=1, **opts))
+            desc = plan.describe()
+            sol = plan.solve()
+            plan.close()
+            assert (sol.value, sol.gray_index) == ref, (opts, desc)
 
 
 def test_plans_sharing_a_kernel_keep_their_shared_memory(ld):
