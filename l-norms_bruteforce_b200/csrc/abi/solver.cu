@@ -72,6 +72,7 @@ struct Choice {
   int PC = 0, multi = 0, i64 = 0;             // wide
   int lane_bits = 0;
   int lin = 0;                                // table: LM column 0 linear in word 0
+  int pair = 0;                               // table: two high indices per thread
 };
 
 int round4(int x) { return (x + 3) & ~3; }
@@ -408,6 +409,19 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     const unsigned long long want = (mine + p->tpb - 1) / p->tpb;
     p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * bps, std::max(1ull, want));
     if (o.blocks > 0) p->blocks = o.blocks;
+    // at least two walks per thread: the instance that walks two high
+    // indices per thread against each table entry read (L_1 / LM, <= 10 words)
+    if (D == 1 && mine >= 2ull * (unsigned long long)p->blocks * (unsigned long long)p->tpb) {
+      const void* pk = ld::table_kernel_pair_ptr(p->ch.WB, p->ch.WA, p->ch.lin);
+      int pbps = 0;
+      if (pk && ld_raise_smem_limit(pk, p->smem) == cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pbps, pk, p->tpb, p->smem) == cudaSuccess && pbps >= 1) {
+        p->kfn = pk;
+        p->ch.pair = 1;
+        if (o.blocks <= 0)
+          p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * pbps, std::max(1ull, want));
+      }
+    }
     // upload image: header | totals | initial H | table bias | packed rows
     std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
     for (int i = 0; i < R; ++i)
@@ -574,8 +588,9 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (!p || !buf) return ld_fail(LD_ERR_ARG, "null argument");
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
-             "table D=%d int32 words=%d int8x4 words=%d lin=%d k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d smem=%zu",
-             p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->k, p->B, p->fw,
+             "table D=%d int32 words=%d int8x4 words=%d lin=%d pair=%d k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d "
+             "smem=%zu",
+             p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->ch.pair, p->k, p->B, p->fw,
              (unsigned long long)p->walks, p->blocks, p->tpb, p->smem);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d", p->ch.PC, p->ch.multi,

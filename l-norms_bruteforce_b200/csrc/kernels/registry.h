@@ -23,8 +23,14 @@ void table_register_dn(TableKernelTab& t);
 using TableKernelLinTab = const void* [3][17];
 void table_register_d1_lin(TableKernelLinTab& t);
 
+// table_kernel<1, WB, WA, LIN, PAIR = true> by (LIN, WB, WA): WB + WA <= 10
+// (LIN only with WB in 1..2)
+using TableKernelPairTab = const void* [2][11][17];
+void table_register_pair(TableKernelPairTab& t);
+
 // nullptr when not instantiated
 const void* table_kernel_mixed_ptr(int D, int WB, int WA);
+const void* table_kernel_pair_ptr(int WB, int WA, int lin);
 const void* table_kernel_lin_ptr(int WB, int WA);
 // all columns in one lane width: PK = 1 (int32, W words) or 4 (int8x4, W words)
 const void* table_kernel_ptr(int D, int W, int PK);

@@ -330,8 +330,38 @@ __device__ __forceinline__ void build_table_dn(const uint32_t* sA, const uint32_
   }
 }
 
+// PAIR instances (L_1 / LM, at most 10 words) walk two high indices per
+// thread against each table entry read, within 64 registers so that 8
+// blocks stay resident per SM; the host uses them when a launch has at
+// least two walks per thread.
+
+// max over all B table entries for two register vectors H and G (two high
+// indices) at once: each entry is read from shared memory once for both.
 template <int D, int WB, int WA, bool LIN = false>
-__global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs args) {
+__device__ __forceinline__ void scan_max2(const uint32_t* H, const uint32_t* G, const uint32_t* sT, int B,
+                                          int& mh, int& mg) {
+  using S = Shape<D, WB, WA>;
+  int m0 = INT_MIN, m1 = INT_MIN;
+  for (int j = 0; j < B; ++j) {
+    const uint4* t = reinterpret_cast<const uint4*>(sT + j * S::NW);
+    uint32_t a0 = 0u, a1 = 0u, b0 = 0u, b1 = 0u;
+#pragma unroll
+    for (int q = 0; q < S::NW / 4; ++q) {
+      const uint4 x = t[q];
+      sad4<D, WB, WA, LIN>(H, x, q, a0, a1);
+      sad4<D, WB, WA, LIN>(G, x, q, b0, b1);
+    }
+    m0 = max(m0, (int)(a0 + a1));
+    m1 = max(m1, (int)(b0 + b1));
+  }
+  if (LIN) { m0 += (int)H[0]; m1 += (int)G[0]; }   // B >= 1: the loop ran
+  mh = m0;
+  mg = m1;
+}
+
+template <int D, int WB, int WA, bool LIN = false, bool PAIR = false>
+__global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(const TableArgs args) {
+  static_assert(!PAIR || (D == 1 && WB + WA <= 10), "paired walks: L_1 / LM with at most 10 words");
   using S = Shape<D, WB, WA>;
   constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
   extern __shared__ __align__(16) uint32_t smem[];
@@ -418,6 +448,32 @@ __global__ void __launch_bounds__(kTableThreads) table_kernel(const TableArgs ar
   uint32_t H[S::NR * WV];
   int best = INT_MIN;
   unsigned long long best_h = 0ull;
+  // Two walks (wk and wk + T) in lockstep when there are at least two walks
+  // per thread: both change the same row at each step (the step depends on
+  // the offset u only), each in its own direction.
+  if constexpr (PAIR) {
+    uint32_t G[WV];
+    for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += 2 * T) {
+      const unsigned long long h0 = wk * WL;
+      const unsigned long long g0 = (wk + T < args.walk_end ? wk + T : wk) * WL;   // a lone walk runs twice
+      seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
+      seed_high<D, WB, WA>(G, sA, sH0, k, nh, g0);
+      for (unsigned long long u = 0; u < WL; ++u) {
+        if (u) {
+          const int i = __ffsll((long long)u) - 1;
+          const int bh = (int)((((h0 + u) >> (i + 1)) & 1ull) ^ 1ull);
+          const int bg = (int)((((g0 + u) >> (i + 1)) & 1ull) ^ 1ull);
+          move_row<D, WB, WA>(H, sA + (k + i) * WT, bh ^ 1, bh);
+          move_row<D, WB, WA>(G, sA + (k + i) * WT, bg ^ 1, bg);
+        }
+        int mh, mg;
+        scan_max2<D, WB, WA, LIN>(H, G, sT, B, mh, mg);
+        // keep the smallest high index among equal maxima
+        if (mh > best || (mh == best && h0 + u < best_h)) { best = mh; best_h = h0 + u; }
+        if (mg > best || (mg == best && g0 + u < best_h)) { best = mg; best_h = g0 + u; }
+      }
+    }
+  } else
   for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += T) {
     const unsigned long long h0 = wk * WL;
     seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);

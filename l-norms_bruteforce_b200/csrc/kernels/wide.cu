@@ -36,6 +36,17 @@ const void* table_kernel_lin_ptr(int WB, int WA) {
   return tab[WB][WA];
 }
 
+const void* table_kernel_pair_ptr(int WB, int WA, int lin) {
+  static TableKernelPairTab tab = {};
+  static bool init = [] {
+    table_register_pair(tab);
+    return true;
+  }();
+  (void)init;
+  if (WB < 0 || WB > 10 || WA < 0 || WA > 16 || WB + WA > 10) return nullptr;
+  return tab[lin ? 1 : 0][WB][WA];
+}
+
 const void* table_kernel_ptr(int D, int W, int PK) {
   if (PK == 1) return table_kernel_mixed_ptr(D, W, 0);
   if (PK == 4) return table_kernel_mixed_ptr(D, 0, W);

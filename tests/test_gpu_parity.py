@@ -289,6 +289,37 @@ def test_plans_sharing_a_kernel_keep_their_shared_memory(ld):
     pb.close()
 
 
+@pytest.mark.parametrize("kind", ["l1", "lm"])
+def test_paired_walks(ld, kind):
+    """Launches with at least two walks per thread use the instance that
+    walks two high indices per thread; value and Gray index match the
+    oracle, also split into 3 shards (uneven walk counts) and with tied rows."""
+    rng = np.random.default_rng(77 if kind == "l1" else 78)
+    if kind == "l1":
+        a = rng.integers(-3, 4, size=(29, 30)).astype(np.int64)
+        a[5] = a[3]
+        marg = False
+    else:
+        a = rng.integers(-2, 3, size=(29, 20)).astype(np.int64)
+        a[:, 0] = rng.integers(-60, 61, size=29)
+        marg = True
+    ref = O.enumerate_max(a, 1, marg)
+    plan = ld.Plan(a, 1, marg)
+    desc = plan.describe()
+    assert "pair=1" in desc, desc
+    if marg:
+        assert "lin=1" in desc, desc
+    sol = plan.solve()
+    plan.close()
+    assert (sol.value, sol.gray_index) == ref, desc
+    best = None
+    for i in range(3):
+        sh = ld.solve_reduced(a, 1, marg, ld.options(shard_index=i, shard_count=3))
+        cand = (sh.value, -sh.gray_index)
+        best = cand if best is None or cand > best else best
+    assert (best[0], -best[1]) == ref
+
+
 def test_lm_linear_column_is_chosen(ld):
     rng = np.random.default_rng(9)
     a = rng.integers(-2, 3, size=(14, 23)).astype(np.int64)
