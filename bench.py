@@ -84,7 +84,7 @@ def issue_ops_per_labeling(desc: str, d: int, cols: int) -> tuple[int, str]:
 # capture summarised in profiles/table_kernel_config2_LM_34x37.md
 # (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is ALU-bound and
 # reads only its matrix image.
-TRAFFIC_BYTES = {2: 36608}
+TRAFFIC_BYTES = {2: 62208}
 
 
 # ---------------------------------------------------------------- clocks
