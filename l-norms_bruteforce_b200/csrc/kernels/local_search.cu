@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "../abi/smem_limit.h"
 #include "../host/ld_internal.h"
 
 namespace {
@@ -35,10 +36,15 @@ struct LsArgs {
 
 __device__ __forceinline__ long long labs64(long long x) { return x < 0 ? -x : x; }
 
+// The block's warps share one copy of the matrix in shared memory (dynamic,
+// R x C int64), staged once: every round of every start reads it.
 __global__ void __launch_bounds__(kLsWarps * 32) local_search_kernel(const LsArgs a) {
+  extern __shared__ long long sA[];
   __shared__ long long sS[kLsWarps][3][kLsMaxCols];
   __shared__ int sLab[kLsWarps][kLsMaxRows];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = threadIdx.x; t < a.R * a.C; t += blockDim.x) sA[t] = a.A[t];
+  __syncthreads();
   const int start = blockIdx.x * kLsWarps + wid;
   if (start >= a.n) return;
   const int R = a.R, C = a.C, d = a.d, nm = d == 1 ? 1 : d;
@@ -50,7 +56,7 @@ __global__ void __launch_bounds__(kLsWarps * 32) local_search_kernel(const LsArg
   for (int l = lane; l < C; l += 32) {
     for (int m = 0; m < nm; ++m) S[m][l] = 0;
     for (int i = 0; i < R; ++i) {
-      const long long x = a.A[(size_t)i * C + l];
+      const long long x = sA[i * C + l];
       if (d == 1) S[0][l] += lab[i] ? x : -x;
       else S[lab[i]][l] += x;
     }
@@ -60,7 +66,7 @@ __global__ void __launch_bounds__(kLsWarps * 32) local_search_kernel(const LsArg
     long long bg = 0;           // best gain of this lane (> 0 to count)
     int bi = INT_MAX, bt = 0;
     for (int i = lane; i < R - 1; i += 32) {
-      const long long* row = a.A + (size_t)i * C;
+      const long long* row = sA + i * C;
       if (d == 1) {
         const long long sg = lab[i] ? -2 : 2;   // change of the column sum per unit of A
         long long g = 0;
@@ -94,7 +100,7 @@ __global__ void __launch_bounds__(kLsWarps * 32) local_search_kernel(const LsArg
     const int from = lab[bi];
     __syncwarp();
     for (int l = lane; l < C; l += 32) {
-      const long long x = a.A[(size_t)bi * C + l];
+      const long long x = sA[bi * C + l];
       if (d == 1) S[0][l] += bt ? 2 * x : -2 * x;
       else { S[from][l] -= x; S[bt][l] += x; }
     }
@@ -167,7 +173,10 @@ extern "C" ld_status ld_local_search(const int64_t* a, int32_t R, int32_t C, int
   LsArgs args{(const long long*)w.dmem, R, C, d, marginal, (const int*)(w.dmem + bA), n,
               max_rounds > 0 ? max_rounds : 4 * R, (long long*)(w.dmem + in_bytes),
               (int*)(w.dmem + in_bytes + bV)};
-  local_search_kernel<<<(n + kLsWarps - 1) / kLsWarps, kLsWarps * 32, 0, w.stream>>>(args);
+  const size_t smem = sizeof(long long) * (size_t)R * C;   // at most 64 rows x 128 columns = 64 KB
+  if (ld_raise_smem_limit((const void*)local_search_kernel, smem) != cudaSuccess)
+    return ld_fail(LD_ERR_CUDA, "local search: cannot reserve %zu bytes of shared memory", smem);
+  local_search_kernel<<<(n + kLsWarps - 1) / kLsWarps, kLsWarps * 32, smem, w.stream>>>(args);
   LS_CUDA(cudaGetLastError());
   LS_CUDA(cudaMemcpyAsync(w.hmem + in_bytes, w.dmem + in_bytes, out_bytes, cudaMemcpyDeviceToHost, w.stream));
   LS_CUDA(cudaStreamSynchronize(w.stream));
