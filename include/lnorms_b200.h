@@ -48,12 +48,16 @@ typedef struct {
     int64_t value;         /* the L_d norm (LM for marginal problems)                */
     uint64_t gray_index;   /* smallest Gray-code index attaining it (tie-break of
                               L_CUDA.cu:80 strict '>' and :347 strict '<')          */
-    uint64_t labelings;    /* labelings the device evaluated or proved dominated    */
+    uint64_t labelings;    /* labelings the solve covered (evaluated, or skipped by
+                              a bound or by label symmetry)                        */
     float kernel_ms;       /* device time of the solve's launches (CUDA events)     */
     int32_t kernel_kind;   /* LD_KERNEL_* actually used                             */
     int32_t lane_bits;     /* 8, 16, 32 or 64: arithmetic lane width used           */
     uint64_t h2d_bytes;    /* host-to-device bytes this solve copied                */
     uint64_t d2h_bytes;    /* device-to-host bytes this solve copied                */
+    uint64_t evaluated;    /* labelings the kernels computed a value for (fewer
+                              than `labelings` when walks were skipped by label
+                              symmetry or by a bound)                              */
 } ld_result;
 
 enum {
@@ -79,6 +83,9 @@ typedef struct {
     int32_t prune_policy;       /* ld_solve_pruned: 0 = run the plain enumeration
                                    instead when more than a quarter of the walk
                                    prefixes survive their bound; 1 = always scan */
+    int32_t enumerate_all;      /* d >= 3: 0 = skip walks that hold no smallest
+                                   index of a label-permutation class (see
+                                   ld_symmetry_walks); 1 = evaluate every walk   */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 
@@ -295,6 +302,20 @@ ld_status ld_tc_gemm(const uint16_t *A, const uint16_t *B, int32_t M, int32_t N,
 /* argument checks, stdout lines and strategy file as L_CUDA's main and     */
 /* arguments_CUDA (L_CUDA.cu:361-439).  Returns the process exit status.    */
 int ld_cli_main(int argc, char **argv);
+
+/* ---------------------------------------------------------------------- */
+/* Label symmetry (d >= 3; the reference enumerates every labeling,         */
+/* L_CUDA.cu:186-240).  The fixed row has label 0 and the value is          */
+/* unchanged when labels 1..d-1 are permuted, so the smallest Gray index     */
+/* attaining the maximum is the smallest index of its class.  A walk of the  */
+/* table kernel fixes the top `prefix_digits` base-d digits of the high      */
+/* index (the walk number w); a walk whose prefix cannot begin a class       */
+/* minimum is skipped (ld_options.enumerate_all = 0).  For d <= 2 every walk */
+/* passes.                                                                   */
+/* 1 when walk w passes the class-minimum test, else 0. */
+int32_t ld_symmetry_walk_ok(int32_t d, int32_t prefix_digits, uint64_t w);
+/* Walks in [lo, hi) that pass (hi <= d^prefix_digits). */
+ld_status ld_symmetry_walks(int32_t d, int32_t prefix_digits, uint64_t lo, uint64_t hi, uint64_t *count);
 
 /* Integer roofline denominator: sustained 32-bit integer ALU operations per
  * second of the device, from a microbenchmark of independent add/xor

@@ -37,14 +37,14 @@ class LdError(RuntimeError):
 class Result(C.Structure):
     _fields_ = [("value", C.c_int64), ("gray_index", C.c_uint64), ("labelings", C.c_uint64),
                 ("kernel_ms", C.c_float), ("kernel_kind", C.c_int32), ("lane_bits", C.c_int32),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("evaluated", C.c_uint64)]
 
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("low_rows", C.c_int32), ("threads_per_block", C.c_int32),
                 ("blocks", C.c_int32), ("tile", C.c_int32), ("kernel", C.c_int32),
                 ("lane_bits", C.c_int32), ("shard_index", C.c_int32), ("shard_count", C.c_int32),
-                ("prune_policy", C.c_int32), ("stream", C.c_void_p)]
+                ("prune_policy", C.c_int32), ("enumerate_all", C.c_int32), ("stream", C.c_void_p)]
 
 
 class ProblemInfo(C.Structure):
@@ -112,6 +112,8 @@ SIGNATURES = [
     ("ld_tc_gemm", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_int32, C.c_int32, C.c_int32,
                              _F32P, C.c_int32]),
     ("ld_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+    ("ld_symmetry_walk_ok", C.c_int32, [C.c_int32, C.c_int32, C.c_uint64]),
+    ("ld_symmetry_walks", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ld_measure_int32_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("ld_last_error", C.c_char_p, []),
     ("ld_version", C.c_char_p, []),
@@ -167,12 +169,13 @@ class Solution:
     lane_bits: int
     h2d_bytes: int = 0
     d2h_bytes: int = 0
+    evaluated: int = 0          # labelings the kernels computed a value for
 
 
 def _solution(res: Result, labels: np.ndarray) -> Solution:
     return Solution(int(res.value), int(res.gray_index), labels, int(res.labelings),
                     float(res.kernel_ms), int(res.kernel_kind), int(res.lane_bits),
-                    int(res.h2d_bytes), int(res.d2h_bytes))
+                    int(res.h2d_bytes), int(res.d2h_bytes), int(res.evaluated))
 
 
 def solve_reduced(a, d: int, marginal: bool = False, opts: Options | None = None) -> Solution:
@@ -242,6 +245,19 @@ def gray_labels(index: int, rows: int, d: int) -> np.ndarray:
     out = np.zeros(max(rows - 1, 1), dtype=np.int32)
     _check(lib().ld_gray_labels(index, rows, d, out.ctypes.data_as(_I32P)))
     return out[: max(rows - 1, 0)]
+
+
+def symmetry_walk_ok(d: int, prefix_digits: int, w: int) -> bool:
+    """Whether walk number w (its top `prefix_digits` base-d digits) can hold
+    the smallest Gray index of a label-permutation class (d >= 3)."""
+    return bool(lib().ld_symmetry_walk_ok(d, prefix_digits, w))
+
+
+def symmetry_walks(d: int, prefix_digits: int, lo: int, hi: int) -> int:
+    """Walk numbers in [lo, hi) that pass symmetry_walk_ok."""
+    n = C.c_uint64()
+    _check(lib().ld_symmetry_walks(d, prefix_digits, lo, hi, C.byref(n)))
+    return int(n.value)
 
 
 def int32_peak(device: int = 0):

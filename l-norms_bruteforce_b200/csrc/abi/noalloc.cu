@@ -197,6 +197,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   args.tbias = nullptr;
   args.R = R; args.k = k; args.B = B; args.fw = fw;
   args.walk_len = walk_len; args.walk_begin = 0; args.walk_end = walks;
+  args.sym_digits = 0; args.sym_pw = 1;   // every walk
   args.value_offset = offset;
   args.red.counter = (unsigned int*)(scratch + kCounter);
   args.red.gvalue = (long long*)(scratch + kGvalue);
@@ -213,6 +214,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   res->value = out.value;
   res->gray_index = out.index;
   res->labelings = walks * walk_len * (unsigned long long)B;
+  res->evaluated = res->labelings;
   res->kernel_kind = LD_KERNEL_TABLE;
   res->lane_bits = 32 / PK;
   res->h2d_bytes = image;

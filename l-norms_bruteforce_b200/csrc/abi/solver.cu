@@ -297,6 +297,9 @@ struct ld_plan {
   Bounds bounds{};
   int k = 0, B = 1, fw = 0;                       // table geometry
   unsigned long long walk_len = 1, walks = 1, walk_begin = 0, walk_end = 1;
+  int sym_digits = 0;                             // label symmetry: walk-number digits tested
+  unsigned long long sym_pw = 1;                  // d^(sym_digits - 1)
+  unsigned long long walks_run = 1;               // walks of [walk_begin, walk_end) that pass
   unsigned long long n_begin = 0, n_end = 0;      // wide geometry
   unsigned long long total = 0;
   int blocks = 1, tpb = 128;
@@ -397,15 +400,36 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     }
     const unsigned long long full = (unsigned long long)di.sms * bps * p->tpb;
     const int nh = F - k;
+    // d >= 3: walks that hold no smallest index of a label-permutation
+    // class are skipped (symmetry.c); the walks that run decide the length
+    const bool sym = D >= 3 && !o.enumerate_all;
+    auto walks_run = [&](int f, unsigned long long lo, unsigned long long hi) -> unsigned long long {
+      uint64_t c = hi - lo;
+      if (sym && nh - f > 0 && ld_symmetry_walks(d, nh - f, lo, hi, &c) != LD_OK) c = hi - lo;
+      return (unsigned long long)c;
+    };
     // walk length: as long as the walks still number >= 32 per thread of a full grid
     int fw = 0;
-    while (fw < nh && ipow(base, nh - fw - 1) >= 32ull * full) ++fw;
+    while (fw < nh && walks_run(fw + 1, 0, ipow(base, nh - fw - 1)) >= 32ull * full) ++fw;
     if (o.tile > 0) fw = std::min(nh, o.tile);
     p->fw = fw;
     p->walk_len = ipow(base, fw);
     p->walks = ipow(base, nh - fw);
-    split_range(p->walks, o.shard_index, o.shard_count, &p->walk_begin, &p->walk_end);
-    const unsigned long long mine = p->walk_end - p->walk_begin;
+    if (sym && nh - fw > 0) {
+      p->sym_digits = nh - fw;
+      p->sym_pw = ipow(base, nh - fw - 1);
+    }
+    if (p->sym_digits > 0 && o.shard_count > 1) {
+      // shards of equal work: equal numbers of walks that pass
+      uint64_t lo = 0, hi = 0;
+      const ld_status sst = ld_sym_split(d, p->sym_digits, o.shard_index, o.shard_count, &lo, &hi);
+      if (sst != LD_OK) { delete p; return sst; }
+      p->walk_begin = lo; p->walk_end = hi;
+    } else {
+      split_range(p->walks, o.shard_index, o.shard_count, &p->walk_begin, &p->walk_end);
+    }
+    p->walks_run = walks_run(fw, p->walk_begin, p->walk_end);
+    const unsigned long long mine = p->walks_run;
     const unsigned long long want = (mine + p->tpb - 1) / p->tpb;
     p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * bps, std::max(1ull, want));
     if (o.blocks > 0) p->blocks = o.blocks;
@@ -504,6 +528,7 @@ static ld_status plan_enqueue(ld_plan* p) {
     args.tbias = (const uint32_t*)(base_ptr + kOffTb);
     args.R = p->R; args.k = p->k; args.B = p->B; args.fw = p->fw;
     args.walk_len = p->walk_len; args.walk_begin = p->walk_begin; args.walk_end = p->walk_end;
+    args.sym_digits = p->sym_digits; args.sym_pw = p->sym_pw;
     args.value_offset = p->value_offset;
     args.red = p->red;
     void* params[] = {&args};
@@ -550,6 +575,8 @@ static ld_status plan_fetch(ld_plan* p, ld_result* res, int32_t* strategy) {
   res->lane_bits = p->ch.lane_bits;
   res->h2d_bytes = p->uploaded ? p->upload_bytes : 0;
   res->d2h_bytes = sizeof(ld::Slot);
+  res->evaluated = p->ch.kind == LD_KERNEL_TABLE ? p->walks_run * p->walk_len * (unsigned long long)p->B
+                                                 : res->labelings;
   if (strategy) ld_gray_labels(res->gray_index, p->R, p->d, strategy);
   p->uploaded = false;
   return LD_OK;
@@ -588,10 +615,11 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (!p || !buf) return ld_fail(LD_ERR_ARG, "null argument");
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
-             "table D=%d int32 words=%d int8x4 words=%d lin=%d pair=%d k=%d B=%d fw=%d walks=%llu blocks=%d tpb=%d "
-             "smem=%zu",
+             "table D=%d int32 words=%d int8x4 words=%d lin=%d pair=%d k=%d B=%d fw=%d walks=%llu run=%llu "
+             "sym=%d blocks=%d tpb=%d smem=%zu",
              p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->ch.pair, p->k, p->B, p->fw,
-             (unsigned long long)p->walks, p->blocks, p->tpb, p->smem);
+             (unsigned long long)p->walks, (unsigned long long)p->walks_run, p->sym_digits, p->blocks, p->tpb,
+             p->smem);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d", p->ch.PC, p->ch.multi,
              p->ch.i64 ? "int64" : "int32", p->blocks, p->tpb);
@@ -829,6 +857,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     t.tbias = (const uint32_t*)(dmem + offTb);
     t.R = R; t.k = k; t.B = B; t.fw = fw;
     t.walk_len = walk_len; t.walk_begin = 0; t.walk_end = walks;
+    t.sym_digits = 0; t.sym_pw = 1;
     t.value_offset = offset;
     t.red.counter = (unsigned int*)(dmem + 0);
     t.red.gvalue = (long long*)(dmem + 8);
@@ -884,6 +913,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
   res->lane_bits = ch.lane_bits;
   res->h2d_bytes = upload;
   res->d2h_bytes = sizeof out + 4 * sizeof(unsigned long long);
+  res->evaluated = hstat[2] * (unsigned long long)B;   // high indices whose block was scanned
   if (strategy) ld_gray_labels(out.index, R, d, strategy);
   ps.pruned = 1;
   ps.walks_kept = hstat[1];

@@ -55,6 +55,10 @@ int ld_max_rows_for(int d);
 /* d^(rows-1) (2^(rows-1) for d <= 2), saturating at UINT64_MAX */
 uint64_t ld_labelings(int rows, int d);
 
+/* walks [lo, hi) of shard `index` of `count`: equal numbers of walks that
+ * pass the label-symmetry test (symmetry.c), tiling [0, d^P) */
+ld_status ld_sym_split(int d, int P, int index, int count, uint64_t *lo, uint64_t *hi);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,9 @@ struct TableArgs {
   int fw;                   // Gray digits walked per seed (walk length d^fw)
   unsigned long long walk_len;
   unsigned long long walk_begin, walk_end;  // walks of this launch
+  int sym_digits;           // D >= 3: digits of the walk number read by the
+                            // label-symmetry test (0 = evaluate every walk)
+  unsigned long long sym_pw;  // D^(sym_digits - 1)
   long long value_offset;   // subtracted from every value (LM shift K)
   Reduce red;
 };
@@ -359,6 +362,43 @@ __device__ __forceinline__ void scan_max2(const uint32_t* H, const uint32_t* G, 
   mg = m1;
 }
 
+// Label symmetry (D >= 3).  The fixed row has label 0 and the value is
+// unchanged when labels 1..D-1 are permuted, so the smallest index attaining
+// the maximum is the smallest index of its class.  Reading the walk number's
+// P digits (the top high digits, fixed along the walk) from the top, the
+// first appearance of each label must take the smallest digit any unseen
+// label could take there: the smallest unseen label where the digit is read
+// directly, the largest where it is mirrored.  Otherwise swapping the two
+// labels leaves the digits above unchanged and lowers this one, i.e. lowers
+// every index of the walk, and the walk holds no class minimum.  With at
+// most one label unseen every continuation passes.  pw = D^(P-1).  The host
+// copy of the test, and the count of the walks that pass, are in symmetry.c.
+template <int D>
+__device__ __forceinline__ bool walk_holds_class_min(unsigned long long wk, int P, unsigned long long pw) {
+  unsigned used = 1u;   // label 0 (the fixed row's) is never moved
+  int seen = 1, par = 0;
+  unsigned long long rem = wk;
+  for (int q = P - 1; q >= 0 && seen < D - 1; --q) {
+    int n = 0;   // digit q: rem < D * pw
+#pragma unroll
+    for (int t = 0; t < D - 1; ++t)
+      if (rem >= pw) { rem -= pw; ++n; }
+    const int lab = par ? D - 1 - n : n;
+    if (!((used >> lab) & 1u)) {
+      const unsigned unused = ~used & ((1u << D) - 1u);
+      const int want = par ? 31 - __clz((int)unused) : __ffs((int)unused) - 1;
+      if (lab != want) return false;
+      used |= 1u << lab;
+      ++seen;
+    }
+    // reflection of the next digit: parity of the number formed by the
+    // digits so far (odd D: of their sum; even D: of the last one)
+    par = (D & 1) ? (par ^ (n & 1)) : (n & 1);
+    pw /= (unsigned long long)D;
+  }
+  return true;
+}
+
 template <int D, int WB, int WA, bool LIN = false, bool PAIR = false>
 __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(const TableArgs args) {
   static_assert(!PAIR || (D == 1 && WB + WA <= 10), "paired walks: L_1 / LM with at most 10 words");
@@ -475,6 +515,9 @@ __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(cons
     }
   } else
   for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += T) {
+    if constexpr (D >= 3) {
+      if (args.sym_digits > 0 && !walk_holds_class_min<D>(wk, args.sym_digits, args.sym_pw)) continue;
+    }
     const unsigned long long h0 = wk * WL;
     seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
     for (unsigned long long u = 0; u < WL; ++u) {
