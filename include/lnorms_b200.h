@@ -260,6 +260,9 @@ ld_status ld_batch_launch(ld_batch *b);
  * *ms = device time of the launch (may be NULL). */
 ld_status ld_batch_results(ld_batch *b, int64_t *values, uint64_t *gray_indices, float *ms);
 ld_status ld_batch_describe(const ld_batch *b, char *buf, size_t cap);
+/* evaluated[count]: labelings the kernels compute a value for, per matrix
+ * (below the matrix's labelings where label symmetry skips walks). */
+ld_status ld_batch_evaluated(const ld_batch *b, uint64_t *evaluated);
 void ld_batch_destroy(ld_batch *b);
 
 /* ---------------------------------------------------------------------- */

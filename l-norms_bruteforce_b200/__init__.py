@@ -90,6 +90,7 @@ SIGNATURES = [
     ("ld_batch_launch", C.c_int, [_P]),
     ("ld_batch_results", C.c_int, [_P, _I64P, C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
     ("ld_batch_describe", C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    ("ld_batch_evaluated", C.c_int, [_P, C.POINTER(C.c_uint64)]),
     ("ld_batch_destroy", None, [_P]),
     ("ld_gray_labels", C.c_int, [C.c_uint64, C.c_int32, C.c_int32, _I32P]),
     ("ld_problem_report", C.c_int, [_P, C.POINTER(Result), _I32P, C.c_int32, _I32P, C.c_char_p, C.c_size_t]),
@@ -471,6 +472,12 @@ class Batch:
         buf = C.create_string_buffer(4096)
         _check(lib().ld_batch_describe(self._h, buf, len(buf)))
         return buf.value.decode()
+
+    def evaluated(self) -> np.ndarray:
+        """Labelings the kernels compute a value for, per matrix (uint64[n])."""
+        e = np.zeros(self.n, dtype=np.uint64)
+        _check(lib().ld_batch_evaluated(self._h, e.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return e
 
     def close(self) -> None:
         if getattr(self, "_h", None):

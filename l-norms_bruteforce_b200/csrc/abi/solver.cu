@@ -555,6 +555,13 @@ static ld_status plan_enqueue(ld_plan* p) {
   return LD_OK;
 }
 
+// labelings the plan's kernel computes a value for
+static unsigned long long plan_evaluated(const ld_plan* p) {
+  if (p->ch.kind == LD_KERNEL_TABLE) return p->walks_run * p->walk_len * (unsigned long long)p->B;
+  if (p->ch.kind == LD_KERNEL_WIDE) return p->n_end - p->n_begin;
+  return 0;
+}
+
 static ld_status plan_fetch(ld_plan* p, ld_result* res, int32_t* strategy) {
   if (!p->launched) return ld_fail(LD_ERR_ARG, "plan has not been launched");
   Resources* r = p->res;
@@ -575,8 +582,7 @@ static ld_status plan_fetch(ld_plan* p, ld_result* res, int32_t* strategy) {
   res->lane_bits = p->ch.lane_bits;
   res->h2d_bytes = p->uploaded ? p->upload_bytes : 0;
   res->d2h_bytes = sizeof(ld::Slot);
-  res->evaluated = p->ch.kind == LD_KERNEL_TABLE ? p->walks_run * p->walk_len * (unsigned long long)p->B
-                                                 : res->labelings;
+  res->evaluated = plan_evaluated(p);
   if (strategy) ld_gray_labels(res->gray_index, p->R, p->d, strategy);
   p->uploaded = false;
   return LD_OK;
@@ -962,6 +968,7 @@ struct ld_batch {
   int n = 0, device = 0;
   std::vector<int> R, C, d, marginal;
   std::vector<unsigned long long> labelings;
+  std::vector<unsigned long long> evaluated;  // labelings the kernels compute a value for
   std::vector<int> cls;                       // class index, or -1 (own plan), or -2 (nothing to do)
   std::vector<ld_plan*> plans;                // per problem, or null
   std::vector<BatchClass> classes;
@@ -1033,6 +1040,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   b->n = count;
   b->device = o.device;
   b->cls.assign(count, -2);
+  b->evaluated.assign(count, 0);
   b->plans.assign(count, nullptr);
   b->range_first.assign(count, 0);
   b->range_end.assign(count, 0);
@@ -1098,6 +1106,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
       if (st != LD_OK) { batch_free(b); return st; }
       b->plans[p] = plan;
       b->cls[p] = -1;
+      b->evaluated[p] = plan_evaluated(plan);
       continue;
     }
     const auto key = std::make_tuple(d, ch.WB, ch.WA);
@@ -1144,6 +1153,16 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     ld::BatchProblem bp{};
     bp.R = R; bp.k = k; bp.B = B; bp.fw = fw;
     bp.walk_len = ipow(base, fw);
+    bp.sym_pw = 1;
+    uint64_t run = walks[p];
+    if (d == 3 && !o.enumerate_all && nh - fw > 0 &&
+        ld_symmetry_walks(d, nh - fw, 0, walks[p], &run) == LD_OK) {
+      bp.sym_digits = nh - fw;
+      bp.sym_pw = ipow(base, nh - fw - 1);
+    } else {
+      run = walks[p];
+    }
+    b->evaluated[p] = (unsigned long long)run * bp.walk_len * (unsigned long long)B;
     bp.value_offset = kh + kl;
     b->hprob.resize(count);
     b->hprob[p] = bp;
@@ -1382,6 +1401,12 @@ extern "C" ld_status ld_batch_results(ld_batch* b, int64_t* values, uint64_t* gr
 extern "C" ld_status ld_batch_describe(const ld_batch* b, char* buf, size_t cap) {
   if (!b || !buf) return ld_fail(LD_ERR_ARG, "null argument");
   snprintf(buf, cap, "%s", b->desc.c_str());
+  return LD_OK;
+}
+
+extern "C" ld_status ld_batch_evaluated(const ld_batch* b, uint64_t* evaluated) {
+  if (!b || !evaluated) return ld_fail(LD_ERR_ARG, "null argument");
+  for (int p = 0; p < b->n; ++p) evaluated[p] = b->evaluated[p];
   return LD_OK;
 }
 

@@ -21,7 +21,9 @@ struct BatchProblem {
   const uint32_t* hinit;    // WT words
   const uint32_t* tbias;    // WT words
   int R, k, B, fw;
+  int sym_digits;           // D = 3: walk-number digits of the label-symmetry test (0 = off)
   unsigned long long walk_len;
+  unsigned long long sym_pw;  // 3^(sym_digits - 1)
   long long value_offset;
 };
 
@@ -148,6 +150,9 @@ __global__ void __launch_bounds__(kBatchThreads) batch_table_kernel(const BatchA
     int best = INT_MIN;
     unsigned long long best_h = 0ull;
     for (unsigned long long wk = ch.walk_begin + threadIdx.x; wk < ch.walk_end; wk += blockDim.x) {
+      if constexpr (D == 3) {   // walks holding no class minimum (table_kernel.cuh)
+        if (pr.sym_digits > 0 && !walk_holds_class_min<3>(wk, pr.sym_digits, pr.sym_pw)) continue;
+      }
       const unsigned long long h0 = wk * WL;
       seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
       for (unsigned long long u = 0; u < WL; ++u) {

@@ -76,3 +76,36 @@ def test_batch_of_config4_sample(ld, workloads):
         sol = ld.solve_reduced(a, d)
         assert (int(v[p]), int(g[p])) == (sol.value, sol.gray_index), p
     b.close()
+
+
+def test_batch_label_symmetry(ld):
+    """d = 3 entries (and a d = 4 own plan) skip the walks that hold no class
+    minimum; values and Gray indices equal the oracle's and the full run's."""
+    rng = np.random.default_rng(31)
+    mats, ds = [], []
+    for t in range(24):
+        r = int(rng.integers(5, 14))
+        if t % 3 == 0:
+            a = rng.choice([-1, 1], size=(r, int(rng.integers(3, 24))))       # many ties
+        elif t % 3 == 1:
+            a = rng.integers(-2, 3, size=(r, int(rng.integers(2, 40))))
+        else:
+            a = rng.integers(-30, 31, size=(r, int(rng.integers(2, 16))))
+            a[1] = a[0]
+        mats.append(np.asarray(a, dtype=np.int64)); ds.append(3)
+    mats.append(rng.integers(-3, 4, size=(8, 12)).astype(np.int64)); ds.append(4)
+    b = ld.Batch(mats, ds)
+    v, g, _ = b.solve()
+    ev = b.evaluated()
+    b.close()
+    full = ld.Batch(mats, ds, opts=ld.options(enumerate_all=1))
+    vf, gf, _ = full.solve()
+    evf = full.evaluated()
+    full.close()
+    for p, (a, d) in enumerate(zip(mats, ds)):
+        ref = O.enumerate_max(a, d, False)
+        assert (int(v[p]), int(g[p])) == ref, (p, a.shape)
+        assert (int(vf[p]), int(gf[p])) == ref, (p, a.shape)
+        assert int(evf[p]) == O.total(a.shape[0], d)
+    big = [p for p, a in enumerate(mats) if a.shape[0] >= 10]
+    assert big and all(ev[p] < evf[p] for p in big)
