@@ -319,6 +319,9 @@ int ld_cli_main(int argc, char **argv);
 int32_t ld_symmetry_walk_ok(int32_t d, int32_t prefix_digits, uint64_t w);
 /* Walks in [lo, hi) that pass (hi <= d^prefix_digits). */
 ld_status ld_symmetry_walks(int32_t d, int32_t prefix_digits, uint64_t lo, uint64_t hi, uint64_t *count);
+/* *w = the passing walk of the given rank (0-based, increasing walk numbers);
+ * the table kernel hands its threads walks by rank. */
+ld_status ld_symmetry_walk_at(int32_t d, int32_t prefix_digits, uint64_t rank, uint64_t *w);
 
 /* Integer roofline denominator: sustained 32-bit integer ALU operations per
  * second of the device, from a microbenchmark of independent add/xor

@@ -115,6 +115,7 @@ SIGNATURES = [
     ("ld_cli_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("ld_symmetry_walk_ok", C.c_int32, [C.c_int32, C.c_int32, C.c_uint64]),
     ("ld_symmetry_walks", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ld_symmetry_walk_at", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ld_measure_int32_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("ld_last_error", C.c_char_p, []),
     ("ld_version", C.c_char_p, []),
@@ -259,6 +260,13 @@ def symmetry_walks(d: int, prefix_digits: int, lo: int, hi: int) -> int:
     n = C.c_uint64()
     _check(lib().ld_symmetry_walks(d, prefix_digits, lo, hi, C.byref(n)))
     return int(n.value)
+
+
+def symmetry_walk_at(d: int, prefix_digits: int, rank: int) -> int:
+    """The passing walk number of the given rank (increasing order)."""
+    w = C.c_uint64()
+    _check(lib().ld_symmetry_walk_at(d, prefix_digits, rank, C.byref(w)))
+    return int(w.value)
 
 
 def int32_peak(device: int = 0):

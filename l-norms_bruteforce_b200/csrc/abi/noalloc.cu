@@ -197,7 +197,8 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   args.tbias = nullptr;
   args.R = R; args.k = k; args.B = B; args.fw = fw;
   args.walk_len = walk_len; args.walk_begin = 0; args.walk_end = walks;
-  args.sym_digits = 0; args.sym_pw = 1;   // every walk
+  args.sym_digits = 0; args.sym_table = nullptr;   // every walk
+  args.rank_begin = args.rank_end = 0;
   args.value_offset = offset;
   args.red.counter = (unsigned int*)(scratch + kCounter);
   args.red.gvalue = (long long*)(scratch + kGvalue);

@@ -297,8 +297,9 @@ struct ld_plan {
   Bounds bounds{};
   int k = 0, B = 1, fw = 0;                       // table geometry
   unsigned long long walk_len = 1, walks = 1, walk_begin = 0, walk_end = 1;
-  int sym_digits = 0;                             // label symmetry: walk-number digits tested
-  unsigned long long sym_pw = 1;                  // d^(sym_digits - 1)
+  int sym_digits = 0;                             // label symmetry: walk-number digits
+  size_t sym_off = 0;                             // completion counts in the device image
+  unsigned long long rank_begin = 0, rank_end = 0;  // passing walks of the shard, by rank
   unsigned long long walks_run = 1;               // walks of [walk_begin, walk_end) that pass
   unsigned long long n_begin = 0, n_end = 0;      // wide geometry
   unsigned long long total = 0;
@@ -415,10 +416,7 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     p->fw = fw;
     p->walk_len = ipow(base, fw);
     p->walks = ipow(base, nh - fw);
-    if (sym && nh - fw > 0) {
-      p->sym_digits = nh - fw;
-      p->sym_pw = ipow(base, nh - fw - 1);
-    }
+    if (sym && nh - fw > 0) p->sym_digits = nh - fw;
     if (p->sym_digits > 0 && o.shard_count > 1) {
       // shards of equal work: equal numbers of walks that pass
       uint64_t lo = 0, hi = 0;
@@ -429,6 +427,10 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
       split_range(p->walks, o.shard_index, o.shard_count, &p->walk_begin, &p->walk_end);
     }
     p->walks_run = walks_run(fw, p->walk_begin, p->walk_end);
+    if (p->sym_digits > 0) {
+      p->rank_begin = walks_run(fw, 0, p->walk_begin);
+      p->rank_end = p->rank_begin + p->walks_run;
+    }
     const unsigned long long mine = p->walks_run;
     const unsigned long long want = (mine + p->tpb - 1) / p->tpb;
     p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * bps, std::max(1ull, want));
@@ -464,7 +466,15 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
       }
     }
     p->upload_bytes = kOffA + (size_t)R * WT * 4;
+    if (p->sym_digits > 0) {   // completion counts for handing out walks by rank
+      p->sym_off = align256(p->upload_bytes);
+      p->upload_bytes = p->sym_off + ld_sym_table_len(d, p->sym_digits) * sizeof(uint64_t);
+    }
     image.assign(p->upload_bytes, 0);
+    if (p->sym_digits > 0) {
+      const ld_status sst = ld_sym_table(d, p->sym_digits, (uint64_t*)(image.data() + p->sym_off));
+      if (sst != LD_OK) { delete p; return sst; }
+    }
     pack_row(tot.data(), p->ch, (uint32_t*)(image.data() + kOffTot));
     pack_row(h0.data(), p->ch, (uint32_t*)(image.data() + kOffH0));
     pack_row(tb.data(), p->ch, (uint32_t*)(image.data() + kOffTb));
@@ -528,7 +538,9 @@ static ld_status plan_enqueue(ld_plan* p) {
     args.tbias = (const uint32_t*)(base_ptr + kOffTb);
     args.R = p->R; args.k = p->k; args.B = p->B; args.fw = p->fw;
     args.walk_len = p->walk_len; args.walk_begin = p->walk_begin; args.walk_end = p->walk_end;
-    args.sym_digits = p->sym_digits; args.sym_pw = p->sym_pw;
+    args.sym_digits = p->sym_digits;
+    args.sym_table = (const unsigned long long*)(base_ptr + p->sym_off);
+    args.rank_begin = p->rank_begin; args.rank_end = p->rank_end;
     args.value_offset = p->value_offset;
     args.red = p->red;
     void* params[] = {&args};
@@ -863,7 +875,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     t.tbias = (const uint32_t*)(dmem + offTb);
     t.R = R; t.k = k; t.B = B; t.fw = fw;
     t.walk_len = walk_len; t.walk_begin = 0; t.walk_end = walks;
-    t.sym_digits = 0; t.sym_pw = 1;
+    t.sym_digits = 0; t.sym_table = nullptr; t.rank_begin = t.rank_end = 0;
     t.value_offset = offset;
     t.red.counter = (unsigned int*)(dmem + 0);
     t.red.gvalue = (long long*)(dmem + 8);

@@ -58,6 +58,11 @@ uint64_t ld_labelings(int rows, int d);
 /* walks [lo, hi) of shard `index` of `count`: equal numbers of walks that
  * pass the label-symmetry test (symmetry.c), tiling [0, d^P) */
 ld_status ld_sym_split(int d, int P, int index, int count, uint64_t *lo, uint64_t *hi);
+/* completion counts f[(used >> 1)][par][r] (ld_sym_table_len entries): the
+ * passing continuations of r more digits after a prefix that has seen the
+ * labels in `used` (bit 0 always set) and whose next digit has reflection par */
+size_t ld_sym_table_len(int d, int P);
+ld_status ld_sym_table(int d, int P, uint64_t *table);
 
 #ifdef __cplusplus
 }

@@ -149,6 +149,67 @@ ld_status ld_symmetry_walks(int32_t d, int32_t P, uint64_t lo, uint64_t hi, uint
     return LD_OK;
 }
 
+size_t ld_sym_table_len(int d, int P) { return ((size_t)1 << (d - 1)) * 2 * (size_t)(P + 1); }
+
+ld_status ld_sym_table(int d, int P, uint64_t *table) {
+    if (d < 3 || d > LD_MAX_D || P <= 0) return ld_fail(LD_ERR_ARG, "no symmetry table for d=%d, %d digits", d, P);
+    sym_ctx c;
+    if (!sym_init(&c, d, P)) return ld_fail(LD_ERR_NOMEM, "symmetry table");
+    for (unsigned u = 1; u < (1u << d); u += 2)
+        for (int par = 0; par < 2; par++)
+            for (int r = 0; r <= P; r++)
+                table[(((size_t)(u >> 1) * 2 + (size_t)par) * (size_t)(P + 1)) + (size_t)r] =
+                    sym_completions(&c, u, par, r);
+    free(c.memo);
+    return LD_OK;
+}
+
+/* The passing walk of a given rank (0-based, increasing walk numbers), from
+ * the completion counts f[(used >> 1)][par][r] of ld_sym_table.  The device
+ * copy is walk_of_rank in table_kernel.cuh. */
+static uint64_t sym_walk_of_rank(int d, int P, const uint64_t *f, uint64_t i) {
+    unsigned used = 1u;
+    int par = 0, q = P - 1;
+    uint64_t w = 0;
+    for (; q >= 0 && sym_free(d, used) > 1; q--) {
+        const int want = sym_want(d, used, par);
+        int n = 0, lab = 0, np = 0;
+        for (n = 0; n < d; n++) {
+            lab = par ? d - 1 - n : n;
+            if (!(((used >> lab) & 1u) || lab == want)) continue;
+            np = sym_next_par(d, par, n);
+            const uint64_t c = f[(((size_t)((used | (1u << lab)) >> 1) * 2 + (size_t)np) * (size_t)(P + 1)) + (size_t)q];
+            if (i < c) break;
+            i -= c;
+        }
+        if (n == d) return UINT64_MAX;   /* rank beyond the passing walks */
+        w = w * (uint64_t)d + (uint64_t)n;
+        used |= 1u << lab;
+        par = np;
+    }
+    /* every suffix of the remaining q + 1 digits passes: in numeric order */
+    for (int t = 0; t <= q; t++) w *= (uint64_t)d;
+    return w + i;
+}
+
+ld_status ld_symmetry_walk_at(int32_t d, int32_t P, uint64_t rank, uint64_t *w) {
+    if (!w) return ld_fail(LD_ERR_ARG, "null output");
+    if (d < 3 || P <= 0) { *w = rank; return LD_OK; }
+    if (d > LD_MAX_D || (double)P * __builtin_log2((double)d) >= 63.0)
+        return ld_fail(LD_ERR_ARG, "prefix of %d base-%d digits", P, d);
+    uint64_t *f = (uint64_t *)malloc(ld_sym_table_len(d, P) * sizeof(uint64_t));
+    if (!f) return ld_fail(LD_ERR_NOMEM, "symmetry table");
+    ld_status st = ld_sym_table(d, P, f);
+    if (st == LD_OK) {
+        const uint64_t K = f[(size_t)0 * (size_t)(P + 1) + (size_t)P];   /* used = {0}, par 0, P digits */
+        if (rank >= K) st = ld_fail(LD_ERR_ARG, "rank %llu of %llu passing walks", (unsigned long long)rank,
+                                    (unsigned long long)K);
+        else *w = sym_walk_of_rank(d, P, f, rank);
+    }
+    free(f);
+    return st;
+}
+
 ld_status ld_sym_split(int d, int P, int index, int count, uint64_t *lo, uint64_t *hi) {
     if (!lo || !hi || count < 1 || index < 0 || index >= count) return ld_fail(LD_ERR_ARG, "bad shard");
     if (d > LD_MAX_D || (double)P * __builtin_log2((double)(d < 2 ? 2 : d)) >= 63.0)

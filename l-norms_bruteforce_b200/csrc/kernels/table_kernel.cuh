@@ -58,8 +58,9 @@ struct TableArgs {
   unsigned long long walk_len;
   unsigned long long walk_begin, walk_end;  // walks of this launch
   int sym_digits;           // D >= 3: digits of the walk number read by the
-                            // label-symmetry test (0 = evaluate every walk)
-  unsigned long long sym_pw;  // D^(sym_digits - 1)
+                            // label symmetry (0 = evaluate every walk)
+  const unsigned long long* sym_table;        // completion counts (walk_of_rank)
+  unsigned long long rank_begin, rank_end;    // passing walks of this launch, by rank
   long long value_offset;   // subtracted from every value (LM shift K)
   Reduce red;
 };
@@ -399,6 +400,41 @@ __device__ __forceinline__ bool walk_holds_class_min(unsigned long long wk, int 
   return true;
 }
 
+// The passing walk of rank i (increasing walk numbers), so that threads take
+// only walks that run, evenly.  f[(used >> 1)][par][r] counts the passing
+// continuations of r more digits after a prefix that has seen the labels in
+// `used` and whose next digit has reflection par (built on the host by the
+// digit DP of symmetry.c, which holds the host copy of this function).  Digit
+// by digit from the top, the digit is the first whose passing continuations
+// reach past i; once at most one label is unseen every continuation passes
+// and the rest of i is the remaining digits.
+template <int D>
+__device__ __forceinline__ unsigned long long walk_of_rank(unsigned long long i, int P,
+                                                           const unsigned long long* __restrict__ f) {
+  unsigned used = 1u;
+  int seen = 1, par = 0, q = P - 1;
+  unsigned long long w = 0;
+  for (; q >= 0 && seen < D - 1; --q) {
+    const unsigned unused = ~used & ((1u << D) - 1u);
+    const int want = par ? 31 - __clz((int)unused) : __ffs((int)unused) - 1;
+    int n = 0, lab = 0, np = 0;
+    for (; n < D; ++n) {
+      lab = par ? D - 1 - n : n;
+      if (!(((used >> lab) & 1u) || lab == want)) continue;
+      np = (D & 1) ? (par ^ (n & 1)) : (n & 1);
+      const unsigned long long c = __ldg(f + ((size_t)((used | (1u << lab)) >> 1) * 2 + np) * (size_t)(P + 1) + q);
+      if (i < c) break;
+      i -= c;
+    }
+    if (n == D) { n = D - 1; lab = par ? 0 : D - 1; np = (D & 1) ? (par ^ (n & 1)) : (n & 1); }  // i past the end
+    w = w * (unsigned long long)D + (unsigned long long)n;
+    if (!((used >> lab) & 1u)) { used |= 1u << lab; ++seen; }
+    par = np;
+  }
+  for (int t = 0; t <= q; ++t) w *= (unsigned long long)D;
+  return w + i;
+}
+
 template <int D, int WB, int WA, bool LIN = false, bool PAIR = false>
 __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(const TableArgs args) {
   static_assert(!PAIR || (D == 1 && WB + WA <= 10), "paired walks: L_1 / LM with at most 10 words");
@@ -513,10 +549,14 @@ __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(cons
         if (mg > best || (mg == best && g0 + u < best_h)) { best = mg; best_h = g0 + u; }
       }
     }
-  } else
-  for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += T) {
+  } else {
+  // d >= 3 with label symmetry: the passing walks, handed out by rank
+  const bool by_rank = D >= 3 && args.sym_digits > 0;
+  const unsigned long long it_end = by_rank ? args.rank_end : args.walk_end;
+  for (unsigned long long it = (by_rank ? args.rank_begin : args.walk_begin) + tid; it < it_end; it += T) {
+    unsigned long long wk = it;
     if constexpr (D >= 3) {
-      if (args.sym_digits > 0 && !walk_holds_class_min<D>(wk, args.sym_digits, args.sym_pw)) continue;
+      if (by_rank) wk = walk_of_rank<D>(it, args.sym_digits, args.sym_table);
     }
     const unsigned long long h0 = wk * WL;
     seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
@@ -555,6 +595,7 @@ __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(cons
       const int m = scan_max<D, WB, WA, LIN>(H, sT, B);
       if (m > best) { best = m; best_h = h0 + u; }
     }
+  }
   }
 
   // The first index attaining the thread's best: rescan its block in the

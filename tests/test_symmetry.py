@@ -173,3 +173,21 @@ def test_library_counts_large_prefixes(ld):
     assert ld.symmetry_walks(2, 40, 5, 17) == 12    # d <= 2: every walk
     with pytest.raises(ld.LdError):
         ld.symmetry_walks(3, 41, 0, 1)              # 3^41 >= 2^63
+
+
+@pytest.mark.parametrize("d,P", [(3, 1), (3, 7), (4, 6), (5, 5), (6, 4), (8, 4), (10, 3)])
+def test_library_walk_of_rank_lists_the_passing_walks(ld, d, P):
+    passing = [w for w in range(d ** P) if walk_ok(w, P, d)]
+    assert [ld.symmetry_walk_at(d, P, r) for r in range(len(passing))] == passing
+    with pytest.raises(ld.LdError):
+        ld.symmetry_walk_at(d, P, len(passing))
+
+
+def test_library_walk_of_rank_long_prefixes(ld):
+    rng = np.random.default_rng(3)
+    for d, P in [(3, 39), (4, 31), (7, 22), (10, 18)]:
+        K = ld.symmetry_walks(d, P, 0, d ** P)
+        for r in [0, 1, K - 1] + [int(x) for x in rng.integers(0, K, size=20)]:
+            w = ld.symmetry_walk_at(d, P, r)
+            assert walk_ok(w, P, d)
+            assert ld.symmetry_walks(d, P, 0, w) == r     # rank = passing walks below it
