@@ -86,6 +86,10 @@ typedef struct {
     int32_t enumerate_all;      /* d >= 3: 0 = skip walks that hold no smallest
                                    index of a label-permutation class (see
                                    ld_symmetry_walks); 1 = evaluate every walk   */
+    int32_t batch_split;        /* ld_batch_create, int32 classes of 40..64 words:
+                                   0 = the autotuner picks the column-split or
+                                   the plain instance (plain when not tuned);
+                                   1 = always column-split; -1 = never          */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

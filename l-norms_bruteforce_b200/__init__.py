@@ -44,7 +44,8 @@ class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("low_rows", C.c_int32), ("threads_per_block", C.c_int32),
                 ("blocks", C.c_int32), ("tile", C.c_int32), ("kernel", C.c_int32),
                 ("lane_bits", C.c_int32), ("shard_index", C.c_int32), ("shard_count", C.c_int32),
-                ("prune_policy", C.c_int32), ("enumerate_all", C.c_int32), ("stream", C.c_void_p)]
+                ("prune_policy", C.c_int32), ("enumerate_all", C.c_int32), ("batch_split", C.c_int32),
+                ("stream", C.c_void_p)]
 
 
 class ProblemInfo(C.Structure):

@@ -965,14 +965,23 @@ struct BatchClass {
   std::vector<int> probs;         // problem indices, largest first
   int wpt = 1;                    // walks per thread per chunk
   double grid_frac = 1.0;         // persistent CTAs per SM, as a fraction of the occupancy limit
+  const void* kfn_split = nullptr;  // column-split instance (wide int32 classes), or null
+  size_t smem_split = 0;
+  int bps_split = 0;
+  bool split = false;             // the autotuner chose the column-split instance
+  float tuned[2] = {0.f, 0.f};    // autotuner: best ms per 1e9 labelings, plain / split instance
+  const void* fn() const { return split ? kfn_split : kfn; }
+  size_t shm() const { return split ? smem_split : smem; }
+  int blocks_per_sm() const { return split ? bps_split : bps; }
   int chunk_first = 0, nchunks = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
 };
 
-// autotuner cache: (D, WB, WA, log2 of the mean walks per problem) -> (wpt, grid fraction)
+// autotuner cache: (D, WB, WA, log2 of the mean walks per problem, batch_split option)
+//   -> (wpt, grid fraction, split)
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int>, std::pair<int, double>> g_tune;
+std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool>> g_tune;
 
 }  // namespace
 
@@ -1130,6 +1139,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
       BatchClass bc;
       bc.D = d; bc.WB = ch.WB; bc.WA = ch.WA;
       bc.kfn = ld::batch_kernel_ptr(d, ch.WB, ch.WA);
+      if (ch.WA == 0 && o.batch_split >= 0) bc.kfn_split = ld::batch_split_kernel_ptr(d, ch.WB);
       b->classes.push_back(bc);
     } else {
       ci = it->second;
@@ -1144,6 +1154,8 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     walks[p] = ipow(base, nh - fw);
     const int B = (int)ipow(base, k), WT = ch.WT;
     bc.smem = std::max(bc.smem, (size_t)ld::table_smem_words(d, WT, R, B) * 4);
+    if (bc.kfn_split)
+      bc.smem_split = std::max(bc.smem_split, (size_t)ld::batch_split_smem_words(d, ch.WB, R, B) * 4);
     // image: tot | h0 | tb | rows (each vector padded to 256 bytes)
     std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
     long long kl = 0, kh = 0;
@@ -1190,6 +1202,13 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
       batch_free(b);
       return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d WA=%d does not fit an SM", c.D, c.WB, c.WA);
+    }
+    if (c.kfn_split && (ld_raise_smem_limit(c.kfn_split, c.smem_split) != cudaSuccess ||
+                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps_split, c.kfn_split, ld::kBatchThreads,
+                                                                      c.smem_split) != cudaSuccess ||
+                        c.bps_split < 1)) {
+      cudaGetLastError();
+      c.kfn_split = nullptr;
     }
   }
   // device memory: images, problem table, chunks (sized for the largest wpt
@@ -1259,7 +1278,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     return args;
   };
   auto class_grid = [&](const BatchClass& c) {
-    const int g = (int)std::max(1.0, std::floor((double)di.sms * c.bps * c.grid_frac));
+    const int g = (int)std::max(1.0, std::floor((double)di.sms * c.blocks_per_sm() * c.grid_frac));
     return std::min(g, std::max(1, c.nchunks));
   };
 
@@ -1270,16 +1289,24 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     double mean = 0;
     for (int p : c.probs) mean += (double)walks[p];
     mean /= std::max<size_t>(1, c.probs.size());
-    const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)));
+    const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)), (int)o.batch_split);
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune.find(key);
-      if (it != g_tune.end()) { c.wpt = it->second.first; c.grid_frac = it->second.second; continue; }
+      if (it != g_tune.end()) {
+        std::tie(c.wpt, c.grid_frac, c.split) = it->second;
+        if (!c.kfn_split) c.split = false;
+        if (o.batch_split > 0 && c.kfn_split) c.split = true;
+        continue;
+      }
     }
+    if (o.batch_split > 0 && c.kfn_split) c.split = true;
     if (!autotune) continue;
     float best_ms = 1e30f;
     int best_wpt = 1;
     double best_frac = 1.0;
+    bool best_split = false;
+    for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
     for (int wpt : {1, 2, 4, 8}) {
       for (double frac : {0.5, 1.0}) {   // persistent CTAs: half or all of the occupancy limit
         std::vector<ld::BatchChunk> all;
@@ -1287,7 +1314,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         // one wave of chunks (a chunk per resident CTA), starting at the
         // class's median matrix: the class's steady state at a fraction of
         // the cost of its largest matrices
-        const int wave = di.sms * c.bps;
+        const int wave = di.sms * (variant ? c.bps_split : c.bps);
         size_t first = 0;
         const int median = c.probs[c.probs.size() / 2];
         while (first < all.size() && all[first].problem != median) ++first;
@@ -1297,7 +1324,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         if (sample < 1) continue;
         cudaMemcpy(b->dmem + b->off_chunks, chunks.data(), sizeof(ld::BatchChunk) * sample, cudaMemcpyHostToDevice);
         BatchClass tc = c;
-        tc.chunk_first = 0; tc.nchunks = sample; tc.grid_frac = frac;
+        tc.chunk_first = 0; tc.nchunks = sample; tc.grid_frac = frac; tc.split = variant == 1;
         ld::BatchArgs args = class_args(c);
         args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks);
         args.nchunks = sample;
@@ -1307,7 +1334,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
           cudaMemsetAsync(args.head, 0, sizeof(unsigned int), b->stream);
           cudaEventRecord(b->ev0, b->stream);
           void* params[] = {&args};
-          cudaLaunchKernel(c.kfn, dim3(class_grid(tc)), dim3(ld::kBatchThreads), params, c.smem, b->stream);
+          cudaLaunchKernel(tc.fn(), dim3(class_grid(tc)), dim3(ld::kBatchThreads), params, tc.shm(), b->stream);
           cudaEventRecord(b->ev1, b->stream);
           cudaEventSynchronize(b->ev1);
           cudaEventElapsedTime(&ms, b->ev0, b->ev1);
@@ -1318,13 +1345,14 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
           lab += (double)(chunks[i].walk_end - chunks[i].walk_begin) * (double)b->hprob[chunks[i].problem].walk_len *
                  (double)b->hprob[chunks[i].problem].B;
         const float per = (float)(ms / std::max(1.0, lab));
-        if (per < best_ms) { best_ms = per; best_wpt = wpt; best_frac = frac; }
+        if (per < best_ms) { best_ms = per; best_wpt = wpt; best_frac = frac; best_split = variant == 1; }
+        if (c.tuned[variant] == 0.f || per * 1e9f < c.tuned[variant]) c.tuned[variant] = per * 1e9f;
       }
     }
     if (cudaGetLastError() != cudaSuccess) { batch_free(b); return ld_fail(LD_ERR_CUDA, "autotune launch failed"); }
-    c.wpt = best_wpt; c.grid_frac = best_frac;
+    c.wpt = best_wpt; c.grid_frac = best_frac; c.split = best_split;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[key] = {best_wpt, best_frac};
+    g_tune[key] = std::make_tuple(best_wpt, best_frac, best_split);
   }
   st = build_queue();
   if (st != LD_OK) { batch_free(b); return st; }
@@ -1340,7 +1368,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     ld::BatchArgs args = class_args(c);
     void* params[] = {&args};
     if (e == cudaSuccess && c.nchunks > 0)
-      e = cudaLaunchKernel(c.kfn, dim3(class_grid(c)), dim3(ld::kBatchThreads), params, c.smem, c.stream);
+      e = cudaLaunchKernel(c.fn(), dim3(class_grid(c)), dim3(ld::kBatchThreads), params, c.shm(), c.stream);
     if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
   }
   ld_status pst = LD_OK;
@@ -1374,9 +1402,13 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
            b->hchunks.size(), (int)std::count_if(b->plans.begin(), b->plans.end(), [](ld_plan* q) { return q != nullptr; }));
   b->desc = buf;
   for (auto& c : b->classes) {
-    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, grid=%d", c.D, c.WB, c.WA,
-             c.probs.size(), c.nchunks, c.wpt, class_grid(c));
+    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, grid=%d%s", c.D, c.WB, c.WA,
+             c.probs.size(), c.nchunks, c.wpt, class_grid(c), c.split ? ", column split" : "");
     b->desc += buf;
+    if (c.tuned[0] > 0.f && c.tuned[1] > 0.f) {
+      snprintf(buf, sizeof buf, " (tuned ms per 1e9 labelings: %.3f, split %.3f)", c.tuned[0], c.tuned[1]);
+      b->desc += buf;
+    }
   }
   *out = b;
   return LD_OK;

@@ -46,6 +46,8 @@ void prune_kernel_ptrs(int D, int WB, int WA, const void** bound, const void** s
 // batch_table_kernel<D, WB, WA> for the batch lane classes (batch_inst.cu), and
 // the per-matrix fold kernel
 const void* batch_kernel_ptr(int D, int WB, int WA);
+// column-split instance of an int32 class (WB = 40, 48, 56, 64), or null
+const void* batch_split_kernel_ptr(int D, int WB);
 const void* batch_fold_kernel_ptr();
 // wide_kernel<IT, PC, MULTI>, PC in {1,2,4,...,128}
 const void* wide_kernel_ptr(int i64, int PC, int multi);

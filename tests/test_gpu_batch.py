@@ -109,3 +109,28 @@ def test_batch_label_symmetry(ld):
         assert int(evf[p]) == O.total(a.shape[0], d)
     big = [p for p, a in enumerate(mats) if a.shape[0] >= 10]
     assert big and all(ev[p] < evf[p] for p in big)
+
+
+@pytest.mark.parametrize("split", [1, -1])
+def test_batch_column_split(ld, split):
+    """Wide int32 classes (40..64 words) on the column-split instances (two
+    threads per high index, one shuffle per entry) and on the plain ones:
+    the oracle's values and Gray indices, d = 1 (and LM), 2, 3, ties."""
+    rng = np.random.default_rng(60 + split)
+    mats, ds, ms = [], [], []
+    for t in range(18):
+        d = 1 + t % 3
+        r = int(rng.integers(4, {1: 16, 2: 15, 3: 10}[d]))
+        c = int(rng.integers(33, 65))
+        a = rng.integers(-300, 301, size=(r, c))
+        if t % 4 == 0:
+            a[1] = a[0]
+        m = int(d == 1 and t % 2 == 0)
+        mats.append(np.asarray(a, dtype=np.int64)); ds.append(d); ms.append(m)
+    b = ld.Batch(mats, ds, ms, opts=ld.options(batch_split=split), autotune=True)
+    desc = b.describe()
+    v, g, _ = b.solve()
+    b.close()
+    assert ("column split" in desc) == (split == 1), desc
+    for p, (a, d, m) in enumerate(zip(mats, ds, ms)):
+        assert (int(v[p]), int(g[p])) == O.enumerate_max(a, d, bool(m)), (p, a.shape, d, m, desc)
