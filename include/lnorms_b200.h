@@ -327,6 +327,18 @@ ld_status ld_symmetry_walks(int32_t d, int32_t prefix_digits, uint64_t lo, uint6
  * the table kernel hands its threads walks by rank. */
 ld_status ld_symmetry_walk_at(int32_t d, int32_t prefix_digits, uint64_t rank, uint64_t *w);
 
+/* ---------------------------------------------------------------------- */
+/* Strategy verifier (no counterpart in the reference).  The value, on the   */
+/* matrix as read, of the labeling a strategy file records (the file of     */
+/* print_results, functions.h:371-412: one entry per input row, or per      */
+/* column when the d = 1 problem was transposed; +1/-1 for d = 1, 0..d-1    */
+/* otherwise).  `text`, d, stat and marginal as for ld_problem_from_text.   */
+ld_status ld_strategy_value(const char *text, size_t len, int32_t d, char stat, int32_t marginal,
+                            const int32_t *strategy, int32_t count, int64_t *value);
+/* `L_verify matrix_file strategy_file d [y|c|r] [m]`: prints the solver's   */
+/* value line ("L3 is: 258") for the strategy; returns the exit status.     */
+int ld_verify_main(int argc, char **argv);
+
 /* Integer roofline denominator: sustained 32-bit integer ALU operations per
  * second of the device, from a microbenchmark of independent add/xor
  * dependency chains (no counterpart in the reference).  *ms gets the

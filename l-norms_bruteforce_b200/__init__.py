@@ -117,6 +117,9 @@ SIGNATURES = [
     ("ld_symmetry_walk_ok", C.c_int32, [C.c_int32, C.c_int32, C.c_uint64]),
     ("ld_symmetry_walks", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ld_symmetry_walk_at", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ld_strategy_value", C.c_int, [C.c_char_p, C.c_size_t, C.c_int32, C.c_char, C.c_int32, _I32P, C.c_int32,
+                                    _I64P]),
+    ("ld_verify_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     ("ld_measure_int32_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("ld_last_error", C.c_char_p, []),
     ("ld_version", C.c_char_p, []),
@@ -268,6 +271,19 @@ def symmetry_walk_at(d: int, prefix_digits: int, rank: int) -> int:
     w = C.c_uint64()
     _check(lib().ld_symmetry_walk_at(d, prefix_digits, rank, C.byref(w)))
     return int(w.value)
+
+
+def strategy_value(text: str, d: int, stat: str = "n", marginal: bool = False, strategy=()) -> int:
+    """The value, on the matrix text as read, of the labeling a strategy
+    file records (one entry per input row, or per column when the d = 1
+    problem is transposed; +1/-1 for d = 1, 0..d-1 otherwise)."""
+    raw = text.encode()
+    lab = np.ascontiguousarray(np.asarray(list(strategy), dtype=np.int32).reshape(-1))
+    buf = lab if lab.size else np.zeros(1, dtype=np.int32)
+    v = C.c_int64()
+    _check(lib().ld_strategy_value(raw, len(raw), d, (stat or "n")[0].encode(), int(marginal),
+                                   buf.ctypes.data_as(_I32P), int(lab.size), C.byref(v)))
+    return int(v.value)
 
 
 def int32_peak(device: int = 0):
