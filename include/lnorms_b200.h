@@ -311,6 +311,24 @@ ld_status ld_tc_gemm(const uint16_t *A, const uint16_t *B, int32_t M, int32_t N,
 int ld_cli_main(int argc, char **argv);
 
 /* ---------------------------------------------------------------------- */
+/* Resumable solves (no counterpart in the reference).  The solve runs as   */
+/* `pieces` shards (ld_options.shard_index / shard_count semantics: equal    */
+/* work per piece) one after another on one device; after each piece the    */
+/* next piece, the Gray range covered and the best (value, index) so far    */
+/* are written to `checkpoint_path` (a small text file, replaced            */
+/* atomically).  A later call with the same matrix, d, marginal, pieces and */
+/* enumerate_all continues after the last recorded piece; a checkpoint of   */
+/* another problem is refused (LD_ERR_ARG), and so is a piece that would    */
+/* not start where the recorded coverage ends (changed options or device).  */
+/* At most max_pieces pieces run per call (<= 0: all).  *done = 1 once every */
+/* piece has run; res (and strategy, rows-1 labels) then hold what          */
+/* ld_solve_reduced gives, with labelings / evaluated / kernel_ms summed    */
+/* over the pieces.  Before that res holds the best so far.                 */
+ld_status ld_solve_resumable(const int64_t *a, int32_t rows, int32_t cols, int32_t d, int32_t marginal,
+                             const ld_options *opt, int32_t pieces, const char *checkpoint_path,
+                             int32_t max_pieces, int32_t *done, ld_result *res, int32_t *strategy);
+
+/* ---------------------------------------------------------------------- */
 /* Label symmetry (d >= 3; the reference enumerates every labeling,         */
 /* L_CUDA.cu:186-240).  The fixed row has label 0 and the value is          */
 /* unchanged when labels 1..d-1 are permuted, so the smallest Gray index     */

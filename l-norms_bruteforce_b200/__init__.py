@@ -117,6 +117,8 @@ SIGNATURES = [
     ("ld_symmetry_walk_ok", C.c_int32, [C.c_int32, C.c_int32, C.c_uint64]),
     ("ld_symmetry_walks", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ld_symmetry_walk_at", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ld_solve_resumable", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
+                                     C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, _I32P]),
     ("ld_strategy_value", C.c_int, [C.c_char_p, C.c_size_t, C.c_int32, C.c_char, C.c_int32, _I32P, C.c_int32,
                                     _I64P]),
     ("ld_verify_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
@@ -208,6 +210,23 @@ def solve_reduced_noalloc(a, d: int, marginal: bool = False, device: int = 0, st
                                           C.c_void_p(stream or None), C.byref(res),
                                           labels.ctypes.data_as(_I32P)))
     return _solution(res, labels[: max(r - 1, 0)])
+
+
+def solve_resumable(a, d: int, marginal: bool = False, pieces: int = 16, checkpoint: str = "",
+                    max_pieces: int = 0, opts: Options | None = None):
+    """Exhaustive solve in `pieces` shards run one after another, with a
+    checkpoint file written after each; a later call with the same matrix
+    and split continues where the file says.  At most `max_pieces` pieces
+    run per call (0: all).  Returns (done, Solution): once done, the
+    Solution equals solve_reduced's; before that it holds the best so far."""
+    a = _as_i64(a)
+    r, c = a.shape
+    labels = np.zeros(max(r - 1, 1), dtype=np.int32)
+    res, done = Result(), C.c_int32()
+    _check(lib().ld_solve_resumable(a.ctypes.data_as(_I64P), r, c, d, int(marginal),
+                                    C.byref(opts) if opts is not None else None, pieces, str(checkpoint).encode(),
+                                    max_pieces, C.byref(done), C.byref(res), labels.ctypes.data_as(_I32P)))
+    return bool(done.value), _solution(res, labels[: max(r - 1, 0)])
 
 
 def local_search(a, d: int, marginal: bool = False, starts=None, n_random: int = 64, seed: int = 0,
