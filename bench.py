@@ -549,7 +549,7 @@ def run_batch(args) -> None:
         mats.append(p.reduced)
         ds.append(info["d"])
         total += int(info["labelings"])
-    opts = ld.options(device=local)
+    opts = ld.options(device=local, batch_split=args.batch_split)
     t0 = time.perf_counter()
     b = ld.Batch(mats, ds, opts=opts, autotune=True)
     create_s = time.perf_counter() - t0
@@ -747,6 +747,9 @@ def main() -> None:
     ap.add_argument("--proposals", type=int, default=8, help="proposals per solve (pruned / learned)")
     ap.add_argument("--count", type=int, default=1,
                     help="pruned / learned: solve this many matrices of the workload's distribution per step")
+    ap.add_argument("--batch-split", type=int, default=0, choices=(-1, 0, 1),
+                    help="config 4: column-split instances of the wide int32 classes "
+                         "(0 = the autotuner picks, 1 = always, -1 = never)")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")
     ap.add_argument("--ref-launch", default="",
