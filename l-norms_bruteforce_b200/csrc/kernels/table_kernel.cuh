@@ -190,28 +190,31 @@ __device__ __forceinline__ void seed_high(uint32_t* H, const uint32_t* sA, const
   }
 }
 
-// Table entry (low labeling) whose labels equal the low rows' labels at
-// Gray index N = h * B + j, for D >= 4.  The low rows' labels are the
-// reflected code's digits 0..k-1 of N; entry e was tabulated with the
-// labels of e's own digits, so e is the inverse of that code applied to
-// these labels (top digit first: a digit's label is mirrored when the
-// number formed by the digits above it is odd).
+// Position j in the block of high index h (N = h * B + j) whose low rows'
+// labels equal those of table entry e, for D >= 4: the inverse of the map
+// from a block position to its table entry.  Entry e was tabulated with the
+// labels of its own digits read alone; the block's low digits are read with
+// the reflection carried down from h (odd h mirrors the top low digit).
+// One pass over the digits from the top recovers e's labels (reflection pe)
+// and j's digits (reflection p, starting at h & 1): a digit's label is
+// mirrored when the number formed by the digits above it is odd (for even D
+// the parity of the digit just above, for odd D of the digit sum).
 template <int D>
-__device__ __forceinline__ int low_entry(unsigned long long N, int k) {
-  int lab[16];
-  unsigned long long q = N;
+__device__ __forceinline__ int block_pos_of_entry(int e, int k, int p0) {
+  int pw = 1;
+  for (int t = 1; t < k; ++t) pw *= D;
+  int j = 0, pe = 0, p = p0, rem = e;
   for (int t = 0; t < k; ++t) {
-    const int r = (int)(q % (2ull * D));
-    lab[t] = r < D ? r : 2 * D - 1 - r;
-    q /= (unsigned long long)D;
+    const int ne = rem / pw;
+    rem -= ne * pw;
+    const int lab = pe ? D - 1 - ne : ne;
+    pe = (D % 2 == 0) ? (ne & 1) : ((pe + ne) & 1);
+    const int n = p ? D - 1 - lab : lab;
+    p = (D % 2 == 0) ? (n & 1) : ((p + n) & 1);
+    j = j * D + n;
+    pw /= D;
   }
-  int e = 0, p = 0;
-  for (int t = k - 1; t >= 0; --t) {
-    const int digit = p ? D - 1 - lab[t] : lab[t];
-    e = e * D + digit;
-    p = (D % 2 == 0) ? (digit & 1) : ((p + digit) & 1);
-  }
-  return e;
+  return j;
 }
 
 // register word compared with table word q (q in [0, NW))
@@ -604,15 +607,24 @@ __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(cons
   unsigned long long bn = ULLONG_MAX;
   if (best != INT_MIN) {
     seed_high<D, WB, WA>(H, sA, sH0, k, nh, best_h);
-    const bool rev = (best_h & 1ull) != 0ull;
-    for (int jj = 0; jj < B; ++jj) {
-      // d <= 3: the low word is read backwards for odd h; D >= 4: the entry
-      // is found from the labels (for even D only the top low digit mirrors)
-      const int je = D >= 4 ? low_entry<(D >= 4 ? D : 4)>(best_h * (unsigned long long)B + (unsigned long long)jj, k)
-                            : (rev ? B - 1 - jj : jj);
-      if (entry_value<D, WB, WA, LIN>(H, sT + je * NW) == best) {
-        bn = best_h * (unsigned long long)B + (unsigned long long)jj;
-        break;
+    if constexpr (D >= 4) {
+      // every entry once, in table order; an entry that attains the best
+      // (rare) is mapped to its block position, and the smallest is kept
+      int jbest = INT_MAX;
+      const int p0 = (int)(best_h & 1ull);
+      for (int je = 0; je < B; ++je)
+        if (entry_value<D, WB, WA, LIN>(H, sT + je * NW) == best)
+          jbest = min(jbest, block_pos_of_entry<D>(je, k, p0));
+      if (jbest != INT_MAX) bn = best_h * (unsigned long long)B + (unsigned long long)jbest;
+    } else {
+      // d <= 3: the low word is read backwards for odd h
+      const bool rev = (best_h & 1ull) != 0ull;
+      for (int jj = 0; jj < B; ++jj) {
+        const int je = rev ? B - 1 - jj : jj;
+        if (entry_value<D, WB, WA, LIN>(H, sT + je * NW) == best) {
+          bn = best_h * (unsigned long long)B + (unsigned long long)jj;
+          break;
+        }
       }
     }
     bv = (long long)best - args.value_offset;

@@ -83,8 +83,8 @@ def reflected_labels(N, ndig, d):
 
 
 def low_entry(N, k, d):
-    """The kernel's low_entry: the isolated low word whose labels equal the
-    low digits' labels of N (table_kernel.cuh)."""
+    """The isolated low word (table entry) whose labels equal the low
+    digits' labels of N; the kernel inverts this map (block_pos_of_entry)."""
     lab = reflected_labels(N, k, d)
     e, p = 0, 0
     for t in range(k - 1, -1, -1):
@@ -114,6 +114,38 @@ def test_low_entry_inverts_the_low_labels(d, k):
             assert reflected_labels(e, k, d) == reflected_labels(N, k, d)
             seen.add(e)
         assert len(seen) == B                        # a bijection for every h
+
+
+def block_pos_of_entry(e, k, p0, d):
+    """The kernel's block_pos_of_entry: the position j in a block of high
+    index h (p0 = h & 1) whose low labels are those of the isolated table
+    entry e; the inverse of low_entry.  One top-down pass over e's digits:
+    e's own labels (reflection pe, the entry read alone) and j's digits
+    (reflection p, starting from the high index's)."""
+    pw = d ** (k - 1) if k > 0 else 1
+    j, pe, p, rem = 0, 0, p0, e
+    for _ in range(k):
+        ne = rem // pw
+        rem -= ne * pw
+        lab = d - 1 - ne if pe else ne
+        pe = (ne & 1) if d % 2 == 0 else ((pe + ne) & 1)
+        n = d - 1 - lab if p else lab
+        p = (n & 1) if d % 2 == 0 else ((p + n) & 1)
+        j = j * d + n
+        pw //= d
+    return j
+
+
+@pytest.mark.parametrize("d,k", [(4, 1), (4, 3), (5, 2), (5, 3), (6, 2), (7, 2), (8, 2), (9, 2), (10, 2), (3, 4)])
+def test_block_pos_inverts_low_entry(d, k):
+    B = d ** k
+    for h in range(0, 4 * d + 3):
+        seen = set()
+        for jj in range(B):
+            e = low_entry(h * B + jj, k, d)
+            assert block_pos_of_entry(e, k, h & 1, d) == jj, (d, k, h, jj)
+            seen.add(e)
+        assert len(seen) == B       # a bijection of the block onto the table
 
 
 @pytest.mark.parametrize("d", [4, 5, 6, 9, 10])
