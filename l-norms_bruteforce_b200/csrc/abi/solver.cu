@@ -481,24 +481,73 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
     for (int i = 0; i < R; ++i)
       pack_row(a + (size_t)i * C, p->ch, (uint32_t*)(image.data() + kOffA) + (size_t)i * WT);
   } else {
-    p->kfn = ld::wide_kernel_ptr(p->ch.i64, p->ch.PC, p->ch.multi);
+    p->kfn = ld::wide_kernel_ptr(p->ch.i64, p->ch.PC, p->ch.multi, 0);
     if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no wide kernel for PC=%d", p->ch.PC); }
     p->tpb = ld::kWideThreads;
     int bps = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, p->kfn, p->tpb, 0) != cudaSuccess || bps < 1) bps = 1;
-    split_range(total, o.shard_index, o.shard_count, &p->n_begin, &p->n_end);
-    const unsigned long long mine = p->n_end - p->n_begin;
     const unsigned long long warps_full = (unsigned long long)di.sms * bps * (p->tpb / 32);
+    // d >= 3: label symmetry over walks of d^L consecutive indices, handed
+    // to warps by rank.  A walk costs a re-seed (R rows) plus its d^L steps;
+    // the slowest warp takes ceil(passing walks / warps) of them.  The walk
+    // length that minimises that estimate is used when it beats evaluating
+    // every index (ceil(labelings / warps) steps plus one seed per warp).
+    // Walks longer than 64 R indices no longer shorten the estimate.
+    int L = -1;
+    if (d >= 3 && !o.enumerate_all && F >= 2) {
+      double best_t = (double)((total + warps_full - 1) / warps_full) + (double)R;
+      for (int l = 0; l <= F - 1 && ipow(d, l) <= 64ull * (unsigned long long)R; ++l) {
+        uint64_t k = 0;
+        if (ld_symmetry_walks(d, F - l, 0, ipow(d, F - l), &k) != LD_OK || k == 0) continue;
+        const double t = std::ceil((double)k / (double)warps_full) * ((double)R + (double)ipow(d, l));
+        if (t < best_t) { best_t = t; L = l; }
+      }
+    }
+    unsigned long long mine = 0;
+    if (L >= 0) {
+      const int P = F - L;
+      p->kfn = ld::wide_kernel_ptr(p->ch.i64, p->ch.PC, p->ch.multi, 1);
+      if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no symmetric wide kernel for PC=%d", p->ch.PC); }
+      p->sym_digits = P;
+      p->walk_len = ipow(d, L);
+      p->walks = ipow(d, P);
+      uint64_t wb = 0, we = p->walks;
+      if (o.shard_count > 1) {
+        const ld_status sst = ld_sym_split(d, P, o.shard_index, o.shard_count, &wb, &we);
+        if (sst != LD_OK) { delete p; return sst; }
+      }
+      uint64_t below = 0, run = 0;
+      if (ld_symmetry_walks(d, P, 0, wb, &below) != LD_OK || ld_symmetry_walks(d, P, wb, we, &run) != LD_OK) {
+        delete p; return ld_fail(LD_ERR_ARG, "symmetry count failed");
+      }
+      p->walk_begin = wb; p->walk_end = we;
+      p->rank_begin = below; p->rank_end = below + run;
+      p->walks_run = run;
+      p->n_begin = wb * p->walk_len;
+      p->n_end = we * p->walk_len;
+      mine = run;
+    } else {
+      split_range(total, o.shard_index, o.shard_count, &p->n_begin, &p->n_end);
+      mine = p->n_end - p->n_begin;
+    }
     const unsigned long long want_warps = std::max(1ull, std::min(warps_full, mine));
     p->blocks = (int)((want_warps + (p->tpb / 32) - 1) / (p->tpb / 32));
     if (o.blocks > 0) p->blocks = o.blocks;
     const size_t esz = p->ch.i64 ? 8 : 4;
     p->upload_bytes = kOffA + (size_t)R * C * esz;
+    if (p->sym_digits > 0) {   // completion counts for handing out walks by rank
+      p->sym_off = align256(p->upload_bytes);
+      p->upload_bytes = p->sym_off + ld_sym_table_len(d, p->sym_digits) * sizeof(uint64_t);
+    }
     image.assign(p->upload_bytes, 0);
     if (p->ch.i64) memcpy(image.data() + kOffA, a, (size_t)R * C * 8);
     else {
       int32_t* dst = (int32_t*)(image.data() + kOffA);
       for (size_t t = 0; t < (size_t)R * C; ++t) dst[t] = (int32_t)a[t];
+    }
+    if (p->sym_digits > 0) {
+      const ld_status sst = ld_sym_table(d, p->sym_digits, (uint64_t*)(image.data() + p->sym_off));
+      if (sst != LD_OK) { delete p; return sst; }
     }
   }
   // scratch header: counter 0, gvalue LLONG_MIN
@@ -550,6 +599,9 @@ static ld_status plan_enqueue(ld_plan* p) {
     args.A = (const long long*)(base_ptr + kOffA);
     args.R = p->R; args.C = p->C; args.d = p->d; args.marginal = p->marginal;
     args.n_begin = p->n_begin; args.n_end = p->n_end;
+    args.sym_digits = p->sym_digits; args.walk_len = p->walk_len;
+    args.sym_table = (const unsigned long long*)(base_ptr + p->sym_off);
+    args.rank_begin = p->rank_begin; args.rank_end = p->rank_end;
     args.red = p->red;
     void* params[] = {&args};
     LD_CUDA(cudaLaunchKernel(p->kfn, dim3(p->blocks), dim3(p->tpb), params, 0, r->stream));
@@ -558,6 +610,9 @@ static ld_status plan_enqueue(ld_plan* p) {
     args.A = (const int*)(base_ptr + kOffA);
     args.R = p->R; args.C = p->C; args.d = p->d; args.marginal = p->marginal;
     args.n_begin = p->n_begin; args.n_end = p->n_end;
+    args.sym_digits = p->sym_digits; args.walk_len = p->walk_len;
+    args.sym_table = (const unsigned long long*)(base_ptr + p->sym_off);
+    args.rank_begin = p->rank_begin; args.rank_end = p->rank_end;
     args.red = p->red;
     void* params[] = {&args};
     LD_CUDA(cudaLaunchKernel(p->kfn, dim3(p->blocks), dim3(p->tpb), params, 0, r->stream));
@@ -570,7 +625,8 @@ static ld_status plan_enqueue(ld_plan* p) {
 // labelings the plan's kernel computes a value for
 static unsigned long long plan_evaluated(const ld_plan* p) {
   if (p->ch.kind == LD_KERNEL_TABLE) return p->walks_run * p->walk_len * (unsigned long long)p->B;
-  if (p->ch.kind == LD_KERNEL_WIDE) return p->n_end - p->n_begin;
+  if (p->ch.kind == LD_KERNEL_WIDE)
+    return p->sym_digits > 0 ? p->walks_run * p->walk_len : p->n_end - p->n_begin;
   return 0;
 }
 
@@ -639,8 +695,9 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
              (unsigned long long)p->walks, (unsigned long long)p->walks_run, p->sym_digits, p->blocks, p->tpb,
              p->smem);
   else
-    snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d", p->ch.PC, p->ch.multi,
-             p->ch.i64 ? "int64" : "int32", p->blocks, p->tpb);
+    snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d sym=%d walk_len=%llu run=%llu", p->ch.PC,
+             p->ch.multi, p->ch.i64 ? "int64" : "int32", p->blocks, p->tpb, p->sym_digits,
+             (unsigned long long)p->walk_len, (unsigned long long)p->walks_run);
   return LD_OK;
 }
 

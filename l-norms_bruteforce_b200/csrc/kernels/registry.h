@@ -50,7 +50,8 @@ const void* batch_kernel_ptr(int D, int WB, int WA);
 const void* batch_split_kernel_ptr(int D, int WB);
 const void* batch_fold_kernel_ptr();
 // wide_kernel<IT, PC, MULTI>, PC in {1,2,4,...,128}
-const void* wide_kernel_ptr(int i64, int PC, int multi);
+// sym = 1: the instance that takes the walks passing the label-symmetry test by rank
+const void* wide_kernel_ptr(int i64, int PC, int multi, int sym);
 
 }  // namespace ld
 

@@ -71,24 +71,30 @@ void prune_kernel_ptrs(int D, int WB, int WA, const void** bound, const void** s
   *scan = prune_kernels()[D][WB][WA][1];
 }
 
-template <typename IT, bool MULTI>
+template <typename IT, bool MULTI, bool SYM>
 static const void* wide_pick(int PC) {
   switch (PC) {
-    case 1: return (const void*)&wide_kernel<IT, 1, MULTI>;
-    case 2: return (const void*)&wide_kernel<IT, 2, MULTI>;
-    case 4: return (const void*)&wide_kernel<IT, 4, MULTI>;
-    case 8: return (const void*)&wide_kernel<IT, 8, MULTI>;
-    case 16: return (const void*)&wide_kernel<IT, 16, MULTI>;
-    case 32: return (const void*)&wide_kernel<IT, 32, MULTI>;
-    case 64: return (const void*)&wide_kernel<IT, 64, MULTI>;
-    case 128: return (const void*)&wide_kernel<IT, 128, MULTI>;
+    case 1: return (const void*)&wide_kernel<IT, 1, MULTI, SYM>;
+    case 2: return (const void*)&wide_kernel<IT, 2, MULTI, SYM>;
+    case 4: return (const void*)&wide_kernel<IT, 4, MULTI, SYM>;
+    case 8: return (const void*)&wide_kernel<IT, 8, MULTI, SYM>;
+    case 16: return (const void*)&wide_kernel<IT, 16, MULTI, SYM>;
+    case 32: return (const void*)&wide_kernel<IT, 32, MULTI, SYM>;
+    case 64: return (const void*)&wide_kernel<IT, 64, MULTI, SYM>;
+    case 128: return (const void*)&wide_kernel<IT, 128, MULTI, SYM>;
     default: return nullptr;
   }
 }
 
-const void* wide_kernel_ptr(int i64, int PC, int multi) {
-  if (i64) return multi ? wide_pick<long long, true>(PC) : wide_pick<long long, false>(PC);
-  return multi ? wide_pick<int, true>(PC) : wide_pick<int, false>(PC);
+// sym: the label-symmetry instance (d >= 3, so multi only)
+const void* wide_kernel_ptr(int i64, int PC, int multi, int sym) {
+  if (sym && !multi) return nullptr;
+  if (i64) {
+    if (sym) return wide_pick<long long, true, true>(PC);
+    return multi ? wide_pick<long long, true, false>(PC) : wide_pick<long long, false, false>(PC);
+  }
+  if (sym) return wide_pick<int, true, true>(PC);
+  return multi ? wide_pick<int, true, false>(PC) : wide_pick<int, false, false>(PC);
 }
 
 }  // namespace ld

@@ -25,6 +25,12 @@ struct WideArgs {
   const IT* A;              // R x C row-major, row R-1 fixed (label 0 / +1)
   int R, C, d, marginal;
   unsigned long long n_begin, n_end;   // Gray indices of this launch
+  // d >= 3 with label symmetry (sym_digits > 0): warps take the walks of
+  // walk_len consecutive indices that pass the class-minimum test, by rank
+  int sym_digits;                      // digits of the walk number
+  unsigned long long walk_len;         // d^(R-1-sym_digits)
+  const unsigned long long* sym_table; // completion counts (table_kernel.cuh walk_of_rank)
+  unsigned long long rank_begin, rank_end;
   Reduce red;
 };
 
@@ -64,19 +70,13 @@ __device__ __forceinline__ void direct_labels(unsigned long long N, int R, int d
 
 // MULTI = false: d == 1 (one signed vector, LM when marginal);
 // MULTI = true:  d >= 2 (d message vectors).
+// The labelings [lo, hi) walked by one warp in Gray order: seeded from
+// lo's labels, then one row moved per index; (bv, bn) keeps the largest
+// value and, among equal values, the first index.
 template <typename IT, int PC, bool MULTI>
-__global__ void __launch_bounds__(kWideThreads) wide_kernel(const WideArgs<IT> args) {
-  const int lane = threadIdx.x & 31;
-  const unsigned long long gw = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+__device__ __forceinline__ void wide_range(const WideArgs<IT>& args, int lane, unsigned long long lo,
+                                           unsigned long long hi, long long& bv, unsigned long long& bn) {
   const int R = args.R, C = args.C, d = args.d;
-  const unsigned long long n = args.n_end - args.n_begin;
-  const unsigned long long steps = n / nw, rem = n % nw;
-  const unsigned long long lo = args.n_begin + gw * steps + (gw < rem ? gw : rem);
-  const unsigned long long hi = lo + steps + (gw < rem ? 1ull : 0ull);
-
-  long long bv = LLONG_MIN;
-  unsigned long long bn = ULLONG_MAX;
   if (lo < hi) {
     int lab[64];
     int dig[65];
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kWideThreads) wide_kernel(const WideArgs<IT> a
       val_lane = (long long)acc;
     }
     long long v = warp_sum<long long>(val_lane);
-    bv = v; bn = lo;
+    if (v > bv) { bv = v; bn = lo; }
     // base-d digits of lo for the step search (d >= 3)
     const int dd = d <= 2 ? 2 : d;
     int dsum = 0;
@@ -169,6 +169,58 @@ __global__ void __launch_bounds__(kWideThreads) wide_kernel(const WideArgs<IT> a
       v = warp_sum<long long>(val_lane);
       if (v > bv) { bv = v; bn = N; }
     }
+  }
+}
+
+// The passing walk of rank i for a runtime order D (the device copy of
+// walk_of_rank in table_kernel.cuh, and of symmetry.c's host copy).
+static __device__ __forceinline__ unsigned long long walk_of_rank_rt(unsigned long long i, int P, int D,
+                                                                  const unsigned long long* __restrict__ f) {
+  unsigned used = 1u;
+  int seen = 1, par = 0, q = P - 1;
+  unsigned long long w = 0;
+  for (; q >= 0 && seen < D - 1; --q) {
+    const unsigned unused = ~used & ((1u << D) - 1u);
+    const int want = par ? 31 - __clz((int)unused) : __ffs((int)unused) - 1;
+    int n = 0, lab = 0, np = 0;
+    for (; n < D; ++n) {
+      lab = par ? D - 1 - n : n;
+      if (!(((used >> lab) & 1u) || lab == want)) continue;
+      np = (D & 1) ? (par ^ (n & 1)) : (n & 1);
+      const unsigned long long c = __ldg(f + ((size_t)((used | (1u << lab)) >> 1) * 2 + np) * (size_t)(P + 1) + q);
+      if (i < c) break;
+      i -= c;
+    }
+    if (n == D) { n = D - 1; lab = par ? 0 : D - 1; np = (D & 1) ? (par ^ (n & 1)) : (n & 1); }  // i past the end
+    w = w * (unsigned long long)D + (unsigned long long)n;
+    if (!((used >> lab) & 1u)) { used |= 1u << lab; ++seen; }
+    par = np;
+  }
+  for (int t = 0; t <= q; ++t) w *= (unsigned long long)D;
+  return w + i;
+}
+
+template <typename IT, int PC, bool MULTI, bool SYM = false>
+__global__ void __launch_bounds__(kWideThreads) wide_kernel(const WideArgs<IT> args) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long gw = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  long long bv = LLONG_MIN;
+  unsigned long long bn = ULLONG_MAX;
+  if constexpr (SYM) {
+    // label symmetry: the passing walks by rank, in increasing index order
+    // per warp
+    for (unsigned long long r = args.rank_begin + gw; r < args.rank_end; r += nw) {
+      const unsigned long long lo = walk_of_rank_rt(r, args.sym_digits, args.d, args.sym_table) * args.walk_len;
+      wide_range<IT, PC, MULTI>(args, lane, lo, lo + args.walk_len, bv, bn);
+    }
+  } else {
+    // one contiguous range per warp
+    const unsigned long long n = args.n_end - args.n_begin;
+    const unsigned long long steps = n / nw, rem = n % nw;
+    const unsigned long long lo = args.n_begin + gw * steps + (gw < rem ? gw : rem);
+    const unsigned long long hi = lo + steps + (gw < rem ? 1ull : 0ull);
+    wide_range<IT, PC, MULTI>(args, lane, lo, hi, bv, bn);
   }
   // one candidate per warp: lane 0's copy (all lanes agree)
   if (lane != 0) { bv = LLONG_MIN; bn = ULLONG_MAX; }

@@ -44,10 +44,11 @@ def test_changed_geometry_is_refused(ld, tmp_path):
     rng = np.random.default_rng(6)
     a = rng.integers(-4, 5, size=(13, 9)).astype(np.int64)
     ck = tmp_path / "solve.ckpt"
-    done, _ = ld.solve_resumable(a, 3, False, pieces=5, checkpoint=ck, max_pieces=1)
+    done, _ = ld.solve_resumable(a, 3, False, pieces=5, checkpoint=ck, max_pieces=1, opts=ld.options(tile=1))
     assert not done
+    # walks of 27 instead of 3 high indices: the pieces' boundaries move
     with pytest.raises(ld.LdError):
-        ld.solve_resumable(a, 3, False, pieces=5, checkpoint=ck, opts=ld.options(kernel=2))
+        ld.solve_resumable(a, 3, False, pieces=5, checkpoint=ck, opts=ld.options(tile=3))
     # the checkpoint is untouched and the original options continue it
-    done, sol = ld.solve_resumable(a, 3, False, pieces=5, checkpoint=ck)
+    done, sol = ld.solve_resumable(a, 3, False, pieces=5, checkpoint=ck, opts=ld.options(tile=1))
     assert done and (sol.value, sol.gray_index) == O.enumerate_max(a, 3, False)

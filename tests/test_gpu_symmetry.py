@@ -85,3 +85,52 @@ def test_symmetric_shards_tile_balance_and_combine(ld, d, count):
     # the shards split the walks that run evenly (to one walk)
     assert sum(work) == whole.evaluated
     assert max(work) - min(work) <= block, (work, block)
+
+
+@pytest.mark.parametrize("d", [3, 4, 5, 6, 8, 10])
+@pytest.mark.parametrize("lanes", [32, 64])
+def test_wide_kernel_symmetry(ld, d, lanes):
+    """The column-parallel kernel hands warps the passing walks by rank: value
+    and index equal the oracle's and the full run's, for 32- and 64-bit sums,
+    on wide and tie-heavy matrices."""
+    rng = np.random.default_rng(900 + 10 * d + lanes)
+    # 1e6 .. 5e6 labelings: enough that walks by rank beat evaluating every
+    # index (the plan's estimate keeps full enumeration for small solves)
+    r = {3: 15, 4: 12, 5: 10, 6: 9, 8: 8, 10: 7}[d]
+    mats = [rng.choice([-1, 1], size=(r, 70)), rng.integers(-3, 4, size=(r, 40))]
+    if lanes == 64:
+        mats.append(rng.integers(-2 ** 40, 2 ** 40, size=(r, 9)))
+    for a in mats:
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        ref = O.enumerate_max(a, d, False)
+        plan = ld.Plan(a, d, False, ld.options(kernel=2, lane_bits=lanes))
+        desc = plan.describe()
+        sol = plan.solve()
+        plan.close()
+        assert (sol.value, sol.gray_index) == ref, desc
+        assert " sym=0 " not in desc and sol.evaluated < sol.labelings, desc
+        full = ld.solve_reduced(a, d, False, ld.options(kernel=2, lane_bits=lanes, enumerate_all=1))
+        assert (full.value, full.gray_index) == ref
+        assert full.evaluated == full.labelings
+
+
+@pytest.mark.parametrize("d,count", [(3, 3), (4, 2), (6, 4)])
+def test_wide_kernel_symmetric_shards(ld, d, count):
+    rng = np.random.default_rng(70 + d)
+    r = {3: 12, 4: 9, 6: 7}[d]
+    a = rng.integers(-5, 6, size=(r, 50)).astype(np.int64)
+    ref = O.enumerate_max(a, d, False)
+    whole = ld.solve_reduced(a, d, False, ld.options(kernel=2))
+    parts, ranges, work = [], [], []
+    for s in range(count):
+        plan = ld.Plan(a, d, False, ld.options(kernel=2, shard_index=s, shard_count=count))
+        ranges.append(plan.range)
+        sol = plan.solve()
+        plan.close()
+        parts.append((sol.value, -sol.gray_index))
+        work.append(sol.evaluated)
+    assert ranges[0][0] == 0 and ranges[-1][1] == O.total(r, d)
+    assert all(ranges[i][1] == ranges[i + 1][0] for i in range(count - 1))
+    best = max(parts)
+    assert (best[0], -best[1]) == ref
+    assert sum(work) == whole.evaluated
