@@ -1064,7 +1064,9 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     t.tbias = (const uint32_t*)(dmem + offTb);
     t.R = R; t.k = k; t.B = B; t.fw = fw;
     t.walk_len = walk_len; t.walk_begin = 0; t.walk_end = walks;
-    t.sym_digits = 0; t.sym_table = nullptr; t.rank_begin = t.rank_end = 0;
+    // d = 3: the walk bound also drops walks that hold no class minimum
+    t.sym_digits = (d == 3 && !o.enumerate_all && nh - fw > 0) ? nh - fw : 0;
+    t.sym_table = nullptr; t.rank_begin = t.rank_end = 0;
     t.value_offset = offset;
     t.red.counter = (unsigned int*)(dmem + 0);
     t.red.gvalue = (long long*)(dmem + 8);

@@ -243,6 +243,11 @@ __global__ void __launch_bounds__(kPruneThreads) walk_bound_kernel(const PruneAr
   const unsigned long long run = (nw + T - 1) / T;
   const unsigned long long first = ta.walk_begin + tid * run;
   uint32_t H[S::NR * S::WV];
+  // d = 3 with label symmetry: a walk that holds no smallest index of a
+  // class (walk_holds_class_min, table_kernel.cuh) is dropped as well
+  const int P = D == 3 ? ta.sym_digits : 0;
+  unsigned long long pw = 1ull;
+  for (int t = 1; t < P; ++t) pw *= 3ull;
   for (unsigned long long r = 0; r < run; ++r) {
     const unsigned long long wk = first + r;
     bool keep = false;
@@ -268,6 +273,9 @@ __global__ void __launch_bounds__(kPruneThreads) walk_bound_kernel(const PruneAr
         move_row<D, WB, WA>(H, sA + (k + fw + i) * S::WT, a, b);
       }
       keep = prefix_abs<D, WB, WA>(H, sTtop) + args.m_walk >= args.threshold;
+      if constexpr (D == 3) {
+        if (P > 0 && keep) keep = walk_holds_class_min<3>(wk, P, pw);
+      }
     }
     const unsigned mask = __ballot_sync(0xffffffffu, keep);
     if (mask) {

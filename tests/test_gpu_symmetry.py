@@ -134,3 +134,22 @@ def test_wide_kernel_symmetric_shards(ld, d, count):
     best = max(parts)
     assert (best[0], -best[1]) == ref
     assert sum(work) == whole.evaluated
+
+
+def test_pruned_search_symmetry(ld):
+    """d = 3 pruned search: the walk bound also drops walks that hold no
+    class minimum; value and index stay the oracle's, and fewer walks are
+    kept than with every walk evaluated."""
+    rng = np.random.default_rng(91)
+    for t in range(4):
+        a = rng.choice([-1, 1], size=(14, 12)) if t % 2 else rng.integers(-3, 4, size=(14, 10))
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        a[4] = a[2]
+        ref = O.enumerate_max(a, 3, False)
+        vals, labs = ld.local_search(a, 3, False, n_random=16, seed=t)
+        inc = labs[int(np.argmax(vals))]
+        sym, st = ld.solve_pruned(a, 3, False, inc, ld.options(prune_policy=1))
+        full, stf = ld.solve_pruned(a, 3, False, inc, ld.options(prune_policy=1, enumerate_all=1))
+        assert (sym.value, sym.gray_index) == ref == (full.value, full.gray_index)
+        assert st["pruned"] == 1 and stf["pruned"] == 1
+        assert st["walks_kept"] < stf["walks_kept"], (st, stf)
