@@ -155,8 +155,15 @@ ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, con
       if (B * (unsigned long long)NW > (o.low_rows >= 0 ? 16384ull : 8192ull)) continue;
       const double words = (double)d * (c.WB + c.WA);
       const double per_lab = words + (2.0 * words + 40.0) / (double)B;
-      const double highs = (double)ipow(base, F - k);
-      const double t = per_lab / std::min(highs, (double)full_threads);
+      // parallel units: the high indices, or (d >= 3, label symmetry) the
+      // ones that can hold a class minimum; time ~ units * B * per_lab
+      // spread over min(units, threads)
+      double units = (double)ipow(base, F - k);
+      if (d >= 3 && !o.enumerate_all && F - k > 0) {
+        uint64_t pass = 0;
+        if (ld_symmetry_walks(d, F - k, 0, ipow(base, F - k), &pass) == LD_OK && pass > 0) units = (double)pass;
+      }
+      const double t = units * (double)B * per_lab / std::min(units, (double)full_threads);
       if (!found || t < best_t * 0.999) { best_t = t; *ch = c; found = true; }
     }
     if (found) return LD_OK;
