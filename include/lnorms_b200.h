@@ -332,17 +332,19 @@ ld_status ld_solve_resumable(const int64_t *a, int32_t rows, int32_t cols, int32
 /* Label symmetry (d >= 3; the reference enumerates every labeling,         */
 /* L_CUDA.cu:186-240).  The fixed row has label 0 and the value is          */
 /* unchanged when labels 1..d-1 are permuted, so the smallest Gray index     */
-/* attaining the maximum is the smallest index of its class.  A walk of the  */
-/* table kernel fixes the top `prefix_digits` base-d digits of the high      */
-/* index (the walk number w); a walk whose prefix cannot begin a class       */
-/* minimum is skipped (ld_options.enumerate_all = 0).  For d <= 2 every walk */
-/* passes.                                                                   */
+/* attaining the maximum is the smallest index of its class.  A walk (the   */
+/* table kernel's block of high indices, the wide kernel's run of d^L       */
+/* consecutive indices) fixes the top `prefix_digits` base-d digits of the  */
+/* index: the walk number w.  A walk whose prefix cannot begin a class      */
+/* minimum is skipped by the table and wide kernels, the batch's d = 3      */
+/* class and the pruned search's walk bound (ld_options.enumerate_all = 0). */
+/* For d <= 2 every walk passes.                                             */
 /* 1 when walk w passes the class-minimum test, else 0. */
 int32_t ld_symmetry_walk_ok(int32_t d, int32_t prefix_digits, uint64_t w);
 /* Walks in [lo, hi) that pass (hi <= d^prefix_digits). */
 ld_status ld_symmetry_walks(int32_t d, int32_t prefix_digits, uint64_t lo, uint64_t hi, uint64_t *count);
 /* *w = the passing walk of the given rank (0-based, increasing walk numbers);
- * the table kernel hands its threads walks by rank. */
+ * the table and wide kernels hand out walks by rank. */
 ld_status ld_symmetry_walk_at(int32_t d, int32_t prefix_digits, uint64_t rank, uint64_t *w);
 
 /* ---------------------------------------------------------------------- */
