@@ -1,0 +1,531 @@
+// Batched solves: one persistent kernel per lane class pulling (matrix, walk
+// range) chunks from a device queue (batch_kernel.cuh); the class kernels
+// run concurrently on forked streams; everything is captured once into a
+// CUDA graph that each ld_batch_launch replays.  Matrices outside the batch
+// lane classes (d >= 4, more columns, 64-bit sums) get their own plans,
+// launched inside the same graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cinttypes>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "smem_limit.h"
+#include "solver_internal.h"
+#include "../kernels/registry.h"
+#include "../kernels/table_kernel.cuh"
+
+using namespace ldsolve;
+
+#include <map>
+#include <tuple>
+
+#include "../kernels/batch_kernel.cuh"
+
+namespace {
+
+struct BatchClass {
+  int D = 0, WB = 0, WA = 0;
+  const void* kfn = nullptr;
+  size_t smem = 0;
+  int bps = 1;
+  std::vector<int> probs;         // problem indices, largest first
+  int wpt = 1;                    // walks per thread per chunk
+  double grid_frac = 1.0;         // persistent CTAs per SM, as a fraction of the occupancy limit
+  const void* kfn_split = nullptr;  // column-split instance (wide int32 classes), or null
+  size_t smem_split = 0;
+  int bps_split = 0;
+  bool split = false;             // the autotuner chose the column-split instance
+  float tuned[2] = {0.f, 0.f};    // autotuner: best ms per 1e9 labelings, plain / split instance
+  const void* fn() const { return split ? kfn_split : kfn; }
+  size_t shm() const { return split ? smem_split : smem; }
+  int blocks_per_sm() const { return split ? bps_split : bps; }
+  int chunk_first = 0, nchunks = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
+// autotuner cache: (D, WB, WA, log2 of the mean walks per problem, batch_split option)
+//   -> (wpt, grid fraction, split)
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool>> g_tune;
+
+}  // namespace
+
+struct ld_batch {
+  int n = 0, device = 0;
+  std::vector<int> R, C, d, marginal;
+  std::vector<unsigned long long> labelings;
+  std::vector<unsigned long long> evaluated;  // labelings the kernels compute a value for
+  std::vector<int> cls;                       // class index, or -1 (own plan), or -2 (nothing to do)
+  std::vector<ld_plan*> plans;                // per problem, or null
+  std::vector<BatchClass> classes;
+  std::vector<ld::BatchProblem> hprob;        // device pointers filled after allocation
+  std::vector<ld::BatchChunk> hchunks;
+  std::vector<int> range_first, range_end;
+  char* dmem = nullptr;
+  size_t off_prob = 0, off_chunks = 0, off_heads = 0, off_cres = 0, off_ranges = 0, off_res = 0;
+  ld::Slot* hres = nullptr;                   // pinned
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool launched = false;
+  std::string desc;
+};
+
+static void batch_free(ld_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto* p : b->plans) if (p) plan_free(p);
+  for (auto& c : b->classes) {
+    if (c.stream) cudaStreamDestroy(c.stream);
+    if (c.done) cudaEventDestroy(c.done);
+  }
+  if (b->dmem) cudaFree(b->dmem);
+  if (b->hres) cudaFreeHost(b->hres);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+// chunks of one class for a given walks-per-thread; returns the number of chunks
+static int batch_chunks(const ld_batch* b, const BatchClass& c, int wpt,
+                        const std::vector<unsigned long long>& walks, std::vector<ld::BatchChunk>* out) {
+  const unsigned long long span = (unsigned long long)ld::kBatchThreads * (unsigned long long)wpt;
+  int n = 0;
+  for (int p : c.probs) {
+    for (unsigned long long w = 0; w < walks[p]; w += span) {
+      ld::BatchChunk ch;
+      ch.walk_begin = w;
+      ch.walk_end = std::min(walks[p], w + span);
+      ch.problem = p;
+      ch.pad = 0;
+      if (out) out->push_back(ch);
+      ++n;
+    }
+  }
+  (void)b;
+  return n;
+}
+
+extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, const int32_t* rows,
+                                     const int32_t* cols, const int32_t* ds, const int32_t* margs,
+                                     const ld_options* opt, int32_t autotune, ld_batch** out) {
+  if (!out || count < 1 || !mats || !rows || !cols || !ds) return ld_fail(LD_ERR_ARG, "bad batch arguments");
+  ld_options o;
+  if (opt) o = *opt; else ld_options_init(&o);
+  DeviceInfo di;
+  ld_status st = device_info(o.device, &di);
+  if (st != LD_OK) return st;
+  if (cudaSetDevice(o.device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "cudaSetDevice failed");
+  ld_batch* b = new ld_batch();
+  b->n = count;
+  b->device = o.device;
+  b->cls.assign(count, -2);
+  b->evaluated.assign(count, 0);
+  b->plans.assign(count, nullptr);
+  b->range_first.assign(count, 0);
+  b->range_end.assign(count, 0);
+  std::vector<unsigned long long> walks(count, 0);
+  std::vector<std::vector<char>> images(count);
+  std::map<std::tuple<int, int, int>, int> class_of;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+    batch_free(b);
+    return ld_fail(LD_ERR_CUDA, "stream/event creation failed");
+  }
+  for (int p = 0; p < count; ++p) {
+    const int R = rows[p], C = cols[p], d = ds[p], marg = margs ? margs[p] : 0;
+    const int64_t* a = mats[p];
+    b->R.push_back(R); b->C.push_back(C); b->d.push_back(d); b->marginal.push_back(marg);
+    if (!a || R < 1 || C < 1 || d < 1 || d > LD_MAX_D || (marg && d != 1) || C > LD_MAX_COLS ||
+        R > ld_max_rows_for(d) || ld_labelings(R, d) >= (1ull << 63)) {
+      batch_free(b);
+      return ld_fail(LD_ERR_ARG, "batch entry %d: invalid or too large (%d x %d, d=%d)", p, R, C, d);
+    }
+    b->labelings.push_back(ld_labelings(R, d));
+    const Bounds bnd = compute_bounds(a, R, C, marg);
+    const bool fits32 = !bnd.overflow && bnd.total + (marg ? bnd.K : 0) <= (long long)INT32_MAX &&
+                        std::max(bnd.colbound, marg ? 2 * bnd.K : 0LL) <= (long long)INT32_MAX;
+    // batch lane class: all columns int8 (WA a multiple of 4) or all int32 (WB a multiple of 8)
+    Choice ch;
+    int k = -1;
+    const int base = d <= 2 ? 2 : d, F = R - 1;
+    if (d <= 3 && fits32 && R >= 2) {
+      for (int kk = std::min(F, 10); kk >= 0; --kk) {
+        const unsigned long long B = ipow(base, kk);
+        if (B > 1024) continue;
+        Choice c;
+        if (!table_config(a, R, C, d, marg, kk, 0, &c)) continue;
+        c.order.clear();
+        for (int l = 0; l < C; ++l) c.order.push_back(l);
+        if (c.WB == 0) { c.WA = round4(c.WA); }
+        else {
+          c.WB = (C + 7) & ~7; c.WA = 0;
+          if (c.WB > 64) continue;
+          // with all-int32 lanes the column order is the identity and every column is wide
+        }
+        c.WT = round4(c.WB + c.WA);
+        if (!ld::batch_kernel_ptr(d, c.WB, c.WA) || B * (unsigned long long)(d * c.WT) > 4096ull) continue;
+        if (c.WB > 0) {      // re-pack every column as int32 (table_config may have put some in int8)
+          c.order.clear();
+          for (int l = 0; l < C; ++l) c.order.push_back(l);
+        } else {
+          // all narrow: table_config's order is identity-compatible
+        }
+        c.lane_bits = c.WB > 0 ? 32 : 8;
+        ch = c; k = kk;
+        break;
+      }
+    }
+    if (k < 0) {                       // own plan, captured in the same graph
+      ld_options po = o;
+      po.stream = b->stream;
+      po.shard_count = 1; po.shard_index = 0;
+      ld_plan* plan = nullptr;
+      st = plan_build(a, R, C, d, marg, &po, nullptr, &plan);
+      if (st != LD_OK) { batch_free(b); return st; }
+      b->plans[p] = plan;
+      b->cls[p] = -1;
+      b->evaluated[p] = plan_evaluated(plan);
+      continue;
+    }
+    const auto key = std::make_tuple(d, ch.WB, ch.WA);
+    auto it = class_of.find(key);
+    int ci;
+    if (it == class_of.end()) {
+      ci = (int)b->classes.size();
+      class_of[key] = ci;
+      BatchClass bc;
+      bc.D = d; bc.WB = ch.WB; bc.WA = ch.WA;
+      bc.kfn = ld::batch_kernel_ptr(d, ch.WB, ch.WA);
+      if (ch.WA == 0 && o.batch_split >= 0) bc.kfn_split = ld::batch_split_kernel_ptr(d, ch.WB);
+      b->classes.push_back(bc);
+    } else {
+      ci = it->second;
+    }
+    b->cls[p] = ci;
+    BatchClass& bc = b->classes[ci];
+    bc.probs.push_back(p);
+    const int nh = F - k;
+    // walks per matrix: at most 2^16 (enough chunks to spread one large matrix)
+    int fw = 0;
+    while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 16.0) ++fw;
+    walks[p] = ipow(base, nh - fw);
+    const int B = (int)ipow(base, k), WT = ch.WT;
+    bc.smem = std::max(bc.smem, (size_t)ld::table_smem_words(d, WT, R, B) * 4);
+    if (bc.kfn_split)
+      bc.smem_split = std::max(bc.smem_split, (size_t)ld::batch_split_smem_words(d, ch.WB, R, B) * 4);
+    // image: tot | h0 | tb | rows (each vector padded to 256 bytes)
+    std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
+    long long kl = 0, kh = 0;
+    for (int i = 0; i < R; ++i)
+      for (int l = 0; l < C; ++l) tot[l] += a[(size_t)i * C + l];
+    if (d == 1) {
+      for (int l = 0; l < C; ++l) h0[l] = a[(size_t)(R - 1) * C + l];
+      if (marg) {
+        for (int i = 0; i < R; ++i) { const int64_t v = a[(size_t)i * C]; (i < k ? kl : kh) += v < 0 ? -v : v; }
+        h0[0] += kh; tb[0] = -kl;
+      }
+    }
+    std::vector<char>& img = images[p];
+    img.assign(768 + align256((size_t)R * WT * 4), 0);
+    pack_row(tot.data(), ch, (uint32_t*)(img.data() + 0));
+    pack_row(h0.data(), ch, (uint32_t*)(img.data() + 256));
+    pack_row(tb.data(), ch, (uint32_t*)(img.data() + 512));
+    for (int i = 0; i < R; ++i) pack_row(a + (size_t)i * C, ch, (uint32_t*)(img.data() + 768) + (size_t)i * WT);
+    ld::BatchProblem bp{};
+    bp.R = R; bp.k = k; bp.B = B; bp.fw = fw;
+    bp.walk_len = ipow(base, fw);
+    bp.sym_pw = 1;
+    uint64_t run = walks[p];
+    if (d == 3 && !o.enumerate_all && nh - fw > 0 &&
+        ld_symmetry_walks(d, nh - fw, 0, walks[p], &run) == LD_OK) {
+      bp.sym_digits = nh - fw;
+      bp.sym_pw = ipow(base, nh - fw - 1);
+    } else {
+      run = walks[p];
+    }
+    b->evaluated[p] = (unsigned long long)run * bp.walk_len * (unsigned long long)B;
+    bp.value_offset = kh + kl;
+    b->hprob.resize(count);
+    b->hprob[p] = bp;
+  }
+  b->hprob.resize(count);
+  // classes: largest matrices first, occupancy, streams
+  for (auto& c : b->classes) {
+    std::stable_sort(c.probs.begin(), c.probs.end(),
+                     [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
+    if (ld_raise_smem_limit(c.kfn, c.smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps, c.kfn, ld::kBatchThreads, c.smem) != cudaSuccess ||
+        c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
+      batch_free(b);
+      return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d WA=%d does not fit an SM", c.D, c.WB, c.WA);
+    }
+    if (c.kfn_split && (ld_raise_smem_limit(c.kfn_split, c.smem_split) != cudaSuccess ||
+                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps_split, c.kfn_split, ld::kBatchThreads,
+                                                                      c.smem_split) != cudaSuccess ||
+                        c.bps_split < 1)) {
+      cudaGetLastError();
+      c.kfn_split = nullptr;
+    }
+  }
+  // device memory: images, problem table, chunks (sized for the largest wpt
+  // candidate = the fewest chunks is wpt 8; the most is wpt 1), heads,
+  // chunk results, ranges, results
+  size_t bytes = 0;
+  std::vector<size_t> img_off(count, 0);
+  for (int p = 0; p < count; ++p)
+    if (b->cls[p] >= 0) { img_off[p] = bytes; bytes += align256(images[p].size()); }
+  int max_chunks = 0;
+  for (auto& c : b->classes) max_chunks += batch_chunks(b, c, 1, walks, nullptr);
+  b->off_prob = bytes;   bytes += align256(sizeof(ld::BatchProblem) * count);
+  b->off_chunks = bytes; bytes += align256(sizeof(ld::BatchChunk) * std::max(1, max_chunks));
+  b->off_heads = bytes;  bytes += align256(sizeof(unsigned int) * std::max<size_t>(1, b->classes.size()));
+  b->off_cres = bytes;   bytes += align256(sizeof(ld::Slot) * std::max(1, max_chunks));
+  b->off_ranges = bytes; bytes += align256(sizeof(int) * 2 * (size_t)count);
+  b->off_res = bytes;    bytes += align256(sizeof(ld::Slot) * count);
+  if (cudaMalloc(&b->dmem, bytes) != cudaSuccess || cudaMallocHost((void**)&b->hres, sizeof(ld::Slot) * count) != cudaSuccess) {
+    batch_free(b);
+    return ld_fail(LD_ERR_CUDA, "batch allocation of %zu bytes failed", bytes);
+  }
+  std::vector<char> hostimg(b->off_prob, 0);
+  for (int p = 0; p < count; ++p) {
+    if (b->cls[p] < 0) continue;
+    memcpy(hostimg.data() + img_off[p], images[p].data(), images[p].size());
+    const char* base_ptr = b->dmem + img_off[p];
+    b->hprob[p].tot = (const uint32_t*)(base_ptr + 0);
+    b->hprob[p].hinit = (const uint32_t*)(base_ptr + 256);
+    b->hprob[p].tbias = (const uint32_t*)(base_ptr + 512);
+    b->hprob[p].A = (const uint32_t*)(base_ptr + 768);
+  }
+  if (cudaMemcpy(b->dmem, hostimg.data(), hostimg.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->dmem + b->off_prob, b->hprob.data(), sizeof(ld::BatchProblem) * count, cudaMemcpyHostToDevice) != cudaSuccess) {
+    batch_free(b);
+    return ld_fail(LD_ERR_CUDA, "batch upload failed");
+  }
+
+  auto build_queue = [&]() -> ld_status {
+    b->hchunks.clear();
+    for (auto& c : b->classes) {
+      c.chunk_first = (int)b->hchunks.size();
+      c.nchunks = batch_chunks(b, c, c.wpt, walks, &b->hchunks);
+    }
+    for (int p = 0; p < count; ++p) { b->range_first[p] = 0; b->range_end[p] = 0; }
+    for (size_t i = 0; i < b->hchunks.size(); ++i) {
+      const int p = b->hchunks[i].problem;
+      if (b->range_end[p] == 0) b->range_first[p] = (int)i;
+      b->range_end[p] = (int)i + 1;
+    }
+    std::vector<int> ranges(2 * (size_t)count);
+    for (int p = 0; p < count; ++p) { ranges[2 * p] = b->range_first[p]; ranges[2 * p + 1] = b->range_end[p]; }
+    if (!b->hchunks.empty() &&
+        cudaMemcpy(b->dmem + b->off_chunks, b->hchunks.data(), sizeof(ld::BatchChunk) * b->hchunks.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return ld_fail(LD_ERR_CUDA, "chunk upload failed");
+    if (cudaMemcpy(b->dmem + b->off_ranges, ranges.data(), sizeof(int) * ranges.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return ld_fail(LD_ERR_CUDA, "range upload failed");
+    return LD_OK;
+  };
+  auto class_args = [&](const BatchClass& c) {
+    ld::BatchArgs args;
+    args.problems = (const ld::BatchProblem*)(b->dmem + b->off_prob);
+    args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks) + c.chunk_first;
+    args.nchunks = c.nchunks;
+    args.head = (unsigned int*)(b->dmem + b->off_heads) + (&c - b->classes.data());
+    args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres) + c.chunk_first;
+    return args;
+  };
+  auto class_grid = [&](const BatchClass& c) {
+    const int g = (int)std::max(1.0, std::floor((double)di.sms * c.blocks_per_sm() * c.grid_frac));
+    return std::min(g, std::max(1, c.nchunks));
+  };
+
+  // autotuner: walks per thread per chunk and the persistent grid size, timed
+  // on one wave of each class's chunks from its median matrix on; cached per
+  // class shape and matrix size.
+  for (auto& c : b->classes) {
+    double mean = 0;
+    for (int p : c.probs) mean += (double)walks[p];
+    mean /= std::max<size_t>(1, c.probs.size());
+    const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)), (int)o.batch_split);
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune.find(key);
+      if (it != g_tune.end()) {
+        std::tie(c.wpt, c.grid_frac, c.split) = it->second;
+        if (!c.kfn_split) c.split = false;
+        if (o.batch_split > 0 && c.kfn_split) c.split = true;
+        continue;
+      }
+    }
+    if (o.batch_split > 0 && c.kfn_split) c.split = true;
+    if (!autotune) continue;
+    float best_ms = 1e30f;
+    int best_wpt = 1;
+    double best_frac = 1.0;
+    bool best_split = false;
+    for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
+    for (int wpt : {1, 2, 4, 8}) {
+      for (double frac : {0.5, 1.0}) {   // persistent CTAs: half or all of the occupancy limit
+        std::vector<ld::BatchChunk> all;
+        batch_chunks(b, c, wpt, walks, &all);
+        // one wave of chunks (a chunk per resident CTA), starting at the
+        // class's median matrix: the class's steady state at a fraction of
+        // the cost of its largest matrices
+        const int wave = di.sms * (variant ? c.bps_split : c.bps);
+        size_t first = 0;
+        const int median = c.probs[c.probs.size() / 2];
+        while (first < all.size() && all[first].problem != median) ++first;
+        if (first + (size_t)wave > all.size()) first = all.size() > (size_t)wave ? all.size() - wave : 0;
+        std::vector<ld::BatchChunk> chunks(all.begin() + first, all.end());
+        const int sample = std::min<int>((int)chunks.size(), wave);
+        if (sample < 1) continue;
+        cudaMemcpy(b->dmem + b->off_chunks, chunks.data(), sizeof(ld::BatchChunk) * sample, cudaMemcpyHostToDevice);
+        BatchClass tc = c;
+        tc.chunk_first = 0; tc.nchunks = sample; tc.grid_frac = frac; tc.split = variant == 1;
+        ld::BatchArgs args = class_args(c);
+        args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks);
+        args.nchunks = sample;
+        args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres);
+        float ms = 0;
+        for (int rep = 0; rep < 1; ++rep) {
+          cudaMemsetAsync(args.head, 0, sizeof(unsigned int), b->stream);
+          cudaEventRecord(b->ev0, b->stream);
+          void* params[] = {&args};
+          cudaLaunchKernel(tc.fn(), dim3(class_grid(tc)), dim3(ld::kBatchThreads), params, tc.shm(), b->stream);
+          cudaEventRecord(b->ev1, b->stream);
+          cudaEventSynchronize(b->ev1);
+          cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        }
+        // normalize by the labelings the sample covered
+        double lab = 0;
+        for (int i = 0; i < sample; ++i)
+          lab += (double)(chunks[i].walk_end - chunks[i].walk_begin) * (double)b->hprob[chunks[i].problem].walk_len *
+                 (double)b->hprob[chunks[i].problem].B;
+        const float per = (float)(ms / std::max(1.0, lab));
+        if (per < best_ms) { best_ms = per; best_wpt = wpt; best_frac = frac; best_split = variant == 1; }
+        if (c.tuned[variant] == 0.f || per * 1e9f < c.tuned[variant]) c.tuned[variant] = per * 1e9f;
+      }
+    }
+    if (cudaGetLastError() != cudaSuccess) { batch_free(b); return ld_fail(LD_ERR_CUDA, "autotune launch failed"); }
+    c.wpt = best_wpt; c.grid_frac = best_frac; c.split = best_split;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = std::make_tuple(best_wpt, best_frac, best_split);
+  }
+  st = build_queue();
+  if (st != LD_OK) { batch_free(b); return st; }
+
+  // capture the whole batch solve into one graph
+  cudaStream_t s = b->stream;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->dmem + b->off_heads, 0, sizeof(unsigned int) * std::max<size_t>(1, b->classes.size()), s);
+  if (e == cudaSuccess) e = cudaEventRecord(b->fork, s);
+  for (auto& c : b->classes) {
+    if (e != cudaSuccess) break;
+    e = cudaStreamWaitEvent(c.stream, b->fork, 0);
+    ld::BatchArgs args = class_args(c);
+    void* params[] = {&args};
+    if (e == cudaSuccess && c.nchunks > 0)
+      e = cudaLaunchKernel(c.fn(), dim3(class_grid(c)), dim3(ld::kBatchThreads), params, c.shm(), c.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
+  }
+  ld_status pst = LD_OK;
+  for (int p = 0; p < count && e == cudaSuccess && pst == LD_OK; ++p)
+    if (b->plans[p]) pst = plan_enqueue(b->plans[p]);
+  for (auto& c : b->classes) if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c.done, 0);
+  if (e == cudaSuccess) {
+    const ld::Slot* cres = (const ld::Slot*)(b->dmem + b->off_cres);
+    const int* ranges = (const int*)(b->dmem + b->off_ranges);
+    ld::Slot* res = (ld::Slot*)(b->dmem + b->off_res);
+    int n = count;
+    void* params[] = {(void*)&cres, (void*)&ranges, (void*)&n, (void*)&res};
+    e = cudaLaunchKernel(ld::batch_fold_kernel_ptr(), dim3((count + 127) / 128), dim3(128), params, 0, s);
+  }
+  for (int p = 0; p < count && e == cudaSuccess; ++p)
+    if (b->plans[p])
+      e = cudaMemcpyAsync(b->dmem + b->off_res + sizeof(ld::Slot) * p, b->plans[p]->red.result, sizeof(ld::Slot),
+                          cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->hres, b->dmem + b->off_res, sizeof(ld::Slot) * count, cudaMemcpyDeviceToHost, s);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  if (e == cudaSuccess) e = e2;
+  b->graph = g;
+  if (e == cudaSuccess && pst == LD_OK) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess || pst != LD_OK) {
+    batch_free(b);
+    return pst != LD_OK ? pst : ld_fail(LD_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
+  }
+  char buf[256];
+  snprintf(buf, sizeof buf, "%d matrices: %zu classes, %zu chunks, %d own plans", count, b->classes.size(),
+           b->hchunks.size(), (int)std::count_if(b->plans.begin(), b->plans.end(), [](ld_plan* q) { return q != nullptr; }));
+  b->desc = buf;
+  for (auto& c : b->classes) {
+    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, grid=%d%s", c.D, c.WB, c.WA,
+             c.probs.size(), c.nchunks, c.wpt, class_grid(c), c.split ? ", column split" : "");
+    b->desc += buf;
+    if (c.tuned[0] > 0.f && c.tuned[1] > 0.f) {
+      snprintf(buf, sizeof buf, " (tuned ms per 1e9 labelings: %.3f, split %.3f)", c.tuned[0], c.tuned[1]);
+      b->desc += buf;
+    }
+  }
+  *out = b;
+  return LD_OK;
+}
+
+extern "C" ld_status ld_batch_launch(ld_batch* b) {
+  if (!b || !b->exec) return ld_fail(LD_ERR_ARG, "null batch");
+  LD_CUDA(cudaSetDevice(b->device));
+  // timing events outside the graph (events recorded during capture cannot be timed)
+  LD_CUDA(cudaEventRecord(b->ev0, b->stream));
+  LD_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  LD_CUDA(cudaEventRecord(b->ev1, b->stream));
+  b->launched = true;
+  return LD_OK;
+}
+
+extern "C" ld_status ld_batch_results(ld_batch* b, int64_t* values, uint64_t* gray_indices, float* ms) {
+  if (!b || !values) return ld_fail(LD_ERR_ARG, "null argument");
+  if (!b->launched) return ld_fail(LD_ERR_ARG, "batch has not been launched");
+  LD_CUDA(cudaSetDevice(b->device));
+  LD_CUDA(cudaStreamSynchronize(b->stream));
+  for (int p = 0; p < b->n; ++p) {
+    values[p] = b->hres[p].value;
+    if (gray_indices) gray_indices[p] = b->hres[p].index;
+  }
+  if (ms) {
+    float t = 0.f;
+    LD_CUDA(cudaEventElapsedTime(&t, b->ev0, b->ev1));
+    *ms = t;
+  }
+  return LD_OK;
+}
+
+extern "C" ld_status ld_batch_describe(const ld_batch* b, char* buf, size_t cap) {
+  if (!b || !buf) return ld_fail(LD_ERR_ARG, "null argument");
+  snprintf(buf, cap, "%s", b->desc.c_str());
+  return LD_OK;
+}
+
+extern "C" ld_status ld_batch_evaluated(const ld_batch* b, uint64_t* evaluated) {
+  if (!b || !evaluated) return ld_fail(LD_ERR_ARG, "null argument");
+  for (int p = 0; p < b->n; ++p) evaluated[p] = b->evaluated[p];
+  return LD_OK;
+}
+
+extern "C" void ld_batch_destroy(ld_batch* b) { batch_free(b); }

@@ -21,31 +21,16 @@
 #include <vector>
 
 #include "smem_limit.h"
-#include "../host/ld_internal.h"
-#include "../kernels/common.cuh"
+#include "solver_internal.h"
 #include "../kernels/registry.h"
 #include "../kernels/table_kernel.cuh"
 #include "../kernels/wide_kernel.cuh"
 
-namespace {
+using namespace ldsolve;
 
-#define LD_CUDA(call)                                                                   \
-  do {                                                                                  \
-    cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess) {                                                            \
-      return ld_fail(e_ == cudaErrorNoDevice || e_ == cudaErrorInsufficientDriver       \
-                         ? LD_ERR_NODEV : LD_ERR_CUDA,                                  \
-                     "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-    }                                                                                   \
-  } while (0)
+namespace ldsolve {
 
-// Exact bounds on every quantity a kernel forms.
-struct Bounds {
-  long long colbound;   // max over columns of sum_i |A_il|: any partial column sum
-  long long total;      // sum of |A_il|: any labeling's value
-  long long K;          // LM: sum_i |A_i0| (column-0 shift)
-  bool overflow;        // a bound itself exceeds int64
-};
+
 
 Bounds compute_bounds(const int64_t* a, int R, int C, int marginal) {
   Bounds b{0, 0, 0, false};
@@ -65,23 +50,8 @@ Bounds compute_bounds(const int64_t* a, int R, int C, int marginal) {
   return b;
 }
 
-struct Choice {
-  int kind = LD_KERNEL_WIDE;
-  int D = 0, WB = 0, WA = 0, WT = 0, k = 0;   // table: int32 words, int8x4 words, padded, low rows
-  std::vector<int> order;                     // table: column of each lane (wide first)
-  int PC = 0, multi = 0, i64 = 0;             // wide
-  int lane_bits = 0;
-  int lin = 0;                                // table: LM column 0 linear in word 0
-  int pair = 0;                               // table: two high indices per thread
-};
 
-int round4(int x) { return (x + 3) & ~3; }
 
-unsigned long long ipow(unsigned long long b, int e) {
-  unsigned long long r = 1;
-  for (int i = 0; i < e; ++i) r *= b;
-  return r;
-}
 
 // Table-kernel configuration for a given number of low rows k: which columns
 // can live in 8-bit lanes.  For d = 1 the two operands of each absolute
@@ -196,11 +166,6 @@ void pack_row(const int64_t* row, const Choice& ch, uint32_t* out) {
     }
 }
 
-struct DeviceInfo {
-  int sms = 148;
-  int max_threads = 1024;
-  bool ok = false;
-};
 
 std::mutex g_dev_mu;
 DeviceInfo g_dev[64];
@@ -224,24 +189,13 @@ ld_status device_info(int dev, DeviceInfo* out) {
   return LD_OK;
 }
 
-}  // namespace
+}  // namespace ldsolve
 
 // ---------------------------------------------------------------------------
-// Device resources: one device arena, a pinned staging buffer, a stream and
-// two events.  A plan owns its own; ld_solve_reduced borrows a per-device
-// workspace so repeated calls allocate nothing after the first.
-namespace {
+// Device resources (solver_internal.h): repeated ld_solve_reduced calls
+// allocate nothing after the first.
+namespace ldsolve {
 
-struct Resources {
-  int device = -1;
-  void* dmem = nullptr;
-  size_t dcap = 0;
-  void* hstage = nullptr;
-  size_t hcap = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
-};
 
 void resources_release(Resources* r) {
   if (r->device < 0) return;
@@ -285,44 +239,16 @@ ld_status resources_acquire(Resources* r, int device, cudaStream_t user_stream, 
 
 std::mutex g_ws_mu[64];
 Resources g_ws[64];
-// per-device workspace of the pruned search (its own stream, arena and
-// pinned result staging), kept between calls
 std::mutex g_pws_mu[64];
 Resources g_pws[64];
 
-constexpr size_t kOffCounter = 0, kOffGvalue = 8, kOffResult = 16;
-constexpr size_t kOffTot = 256, kOffH0 = 512, kOffTb = 768, kOffA = 1024;
 
-size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-}  // namespace
 
-struct ld_plan {
-  int device = 0;
-  int R = 0, C = 0, d = 0, marginal = 0;
-  Choice ch;
-  Bounds bounds{};
-  int k = 0, B = 1, fw = 0;                       // table geometry
-  unsigned long long walk_len = 1, walks = 1, walk_begin = 0, walk_end = 1;
-  int sym_digits = 0;                             // label symmetry: walk-number digits
-  size_t sym_off = 0;                             // completion counts in the device image
-  unsigned long long rank_begin = 0, rank_end = 0;  // passing walks of the shard, by rank
-  unsigned long long walks_run = 1;               // walks of [walk_begin, walk_end) that pass
-  unsigned long long n_begin = 0, n_end = 0;      // wide geometry
-  unsigned long long total = 0;
-  int blocks = 1, tpb = 128;
-  size_t smem = 0;
-  long long value_offset = 0;
-  Resources own;
-  Resources* res = nullptr;
-  size_t upload_bytes = 0;
-  bool uploaded = false;       // the upload belongs to the next fetched launch
-  ld::Reduce red{};
-  const void* kfn = nullptr;
-  bool launched = false;
-};
+}  // namespace ldsolve
 
-static void plan_free(ld_plan* p) {
+
+void ldsolve::plan_free(ld_plan* p) {
   if (!p) return;
   if (p->res == &p->own) resources_release(&p->own);
   delete p;
@@ -344,7 +270,7 @@ extern "C" int ld_device_max_threads(int device, int* out) {
 }
 
 // Split [0, n) into `count` contiguous parts; part `idx` (calc_jmin_jmax form).
-static void split_range(unsigned long long n, int idx, int count, unsigned long long* lo,
+void ldsolve::split_range(unsigned long long n, int idx, int count, unsigned long long* lo,
                         unsigned long long* hi) {
   if (count <= 1) { *lo = 0; *hi = n; return; }
   const unsigned long long c = (unsigned long long)count, i = (unsigned long long)idx;
@@ -356,7 +282,7 @@ static void split_range(unsigned long long n, int idx, int count, unsigned long 
 // Geometry, kernel choice and the upload image; resources are attached by
 // the caller.  `shared` selects the per-device workspace instead of owned
 // resources.
-static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal, const ld_options* opt,
+ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int marginal, const ld_options* opt,
                             Resources* shared, ld_plan** out) {
   ld_options o;
   if (opt) o = *opt; else ld_options_init(&o);
@@ -585,7 +511,7 @@ static ld_status plan_build(const int64_t* a, int R, int C, int d, int marginal,
   return LD_OK;
 }
 
-static ld_status plan_enqueue(ld_plan* p) {
+ld_status ldsolve::plan_enqueue(ld_plan* p) {
   Resources* r = p->res;
   char* base_ptr = (char*)r->dmem;
   LD_CUDA(cudaSetDevice(p->device));
@@ -634,14 +560,14 @@ static ld_status plan_enqueue(ld_plan* p) {
 }
 
 // labelings the plan's kernel computes a value for
-static unsigned long long plan_evaluated(const ld_plan* p) {
+unsigned long long ldsolve::plan_evaluated(const ld_plan* p) {
   if (p->ch.kind == LD_KERNEL_TABLE) return p->walks_run * p->walk_len * (unsigned long long)p->B;
   if (p->ch.kind == LD_KERNEL_WIDE)
     return p->sym_digits > 0 ? p->walks_run * p->walk_len : p->n_end - p->n_begin;
   return 0;
 }
 
-static ld_status plan_fetch(ld_plan* p, ld_result* res, int32_t* strategy) {
+ld_status ldsolve::plan_fetch(ld_plan* p, ld_result* res, int32_t* strategy) {
   if (!p->launched) return ld_fail(LD_ERR_ARG, "plan has not been launched");
   Resources* r = p->res;
   LD_CUDA(cudaSetDevice(p->device));
@@ -736,924 +662,3 @@ extern "C" ld_status ld_solve_reduced(const int64_t* a, int32_t rows, int32_t co
   return st;
 }
 
-// ---------------------------------------------------------------------------
-// Resumable solves: the shards of one solve run one after another, with a
-// checkpoint after each (no counterpart in the reference, whose runs cannot
-// be interrupted and resumed).
-namespace {
-
-// FNV-1a over the problem and the split, so that a checkpoint is only ever
-// continued by the solve that wrote it
-unsigned long long checkpoint_fingerprint(const int64_t* a, int R, int C, int d, int marginal, int pieces,
-                                          int enumerate_all) {
-  unsigned long long h = 1469598103934665603ull;
-  auto mix = [&](const void* p, size_t n) {
-    const unsigned char* c = (const unsigned char*)p;
-    for (size_t i = 0; i < n; ++i) { h ^= c[i]; h *= 1099511628211ull; }
-  };
-  const int hdr[6] = {R, C, d, marginal, pieces, enumerate_all};
-  mix(hdr, sizeof hdr);
-  mix(a, (size_t)R * C * sizeof(int64_t));
-  return h;
-}
-
-struct Checkpoint {
-  unsigned long long fingerprint = 0;
-  int pieces = 0, next = 0;
-  unsigned long long covered = 0;             // Gray indices [0, covered) are done
-  long long value = LLONG_MIN;                // best so far (LLONG_MIN: none)
-  unsigned long long index = ULLONG_MAX;
-  unsigned long long labelings = 0, evaluated = 0;
-  double kernel_ms = 0;
-};
-
-// 1 = read, 0 = no file, -1 = unreadable
-int checkpoint_read(const char* path, Checkpoint* ck) {
-  FILE* f = fopen(path, "r");
-  if (!f) return 0;
-  int version = 0;
-  const int n = fscanf(f, "lnorms-checkpoint %d fingerprint %llx pieces %d next %d covered %llu value %lld index %llu "
-                          "labelings %llu evaluated %llu kernel_ms %lf",
-                       &version, &ck->fingerprint, &ck->pieces, &ck->next, &ck->covered, &ck->value, &ck->index,
-                       &ck->labelings, &ck->evaluated, &ck->kernel_ms);
-  fclose(f);
-  return (n == 10 && version == 1) ? 1 : -1;
-}
-
-bool checkpoint_write(const char* path, const Checkpoint& ck) {
-  const std::string tmp = std::string(path) + ".tmp";
-  FILE* f = fopen(tmp.c_str(), "w");
-  if (!f) return false;
-  const int n = fprintf(f,
-                        "lnorms-checkpoint 1\nfingerprint %016llx\npieces %d\nnext %d\ncovered %llu\nvalue %lld\n"
-                        "index %llu\nlabelings %llu\nevaluated %llu\nkernel_ms %.6f\n",
-                        ck.fingerprint, ck.pieces, ck.next, ck.covered, ck.value, ck.index, ck.labelings,
-                        ck.evaluated, ck.kernel_ms);
-  const bool ok = n > 0 && fflush(f) == 0;
-  if (fclose(f) != 0 || !ok) return false;
-  return rename(tmp.c_str(), path) == 0;   // the old checkpoint stays valid until here
-}
-
-}  // namespace
-
-extern "C" ld_status ld_solve_resumable(const int64_t* a, int32_t rows, int32_t cols, int32_t d, int32_t marginal,
-                                        const ld_options* opt, int32_t pieces, const char* checkpoint_path,
-                                        int32_t max_pieces, int32_t* done, ld_result* res, int32_t* strategy) {
-  if (!a || !checkpoint_path || !done || !res) return ld_fail(LD_ERR_ARG, "null argument");
-  if (rows < 1 || cols < 1 || d < 1 || d > LD_MAX_D) return ld_fail(LD_ERR_ARG, "bad problem %d x %d, d=%d", rows, cols, d);
-  if (pieces < 1) return ld_fail(LD_ERR_ARG, "pieces must be >= 1 (got %d)", pieces);
-  ld_options o;
-  if (opt) o = *opt; else ld_options_init(&o);
-  if (o.shard_count > 1) return ld_fail(LD_ERR_ARG, "a resumable solve makes its own shards");
-  const int marg = d == 1 && marginal ? 1 : 0;
-  const unsigned long long fp = checkpoint_fingerprint(a, rows, cols, d, marg, pieces, o.enumerate_all ? 1 : 0);
-  Checkpoint ck;
-  const int got = checkpoint_read(checkpoint_path, &ck);
-  if (got < 0) return ld_fail(LD_ERR_IO, "%s is not a checkpoint of this library", checkpoint_path);
-  if (got == 0) {
-    ck = Checkpoint();
-    ck.fingerprint = fp;
-    ck.pieces = pieces;
-  } else if (ck.fingerprint != fp || ck.pieces != pieces) {
-    return ld_fail(LD_ERR_ARG, "%s belongs to another problem or split (fingerprint %016llx, %d pieces)",
-                   checkpoint_path, ck.fingerprint, ck.pieces);
-  } else if (ck.next < 0 || ck.next > pieces) {
-    return ld_fail(LD_ERR_IO, "%s records piece %d of %d", checkpoint_path, ck.next, pieces);
-  }
-  int ran = 0;
-  int kind = LD_KERNEL_NONE, lane_bits = 0;
-  while (ck.next < pieces && (max_pieces <= 0 || ran < max_pieces)) {
-    ld_options po = o;
-    po.shard_index = ck.next;
-    po.shard_count = pieces;
-    ld_plan* p = nullptr;
-    ld_status st = ld_plan_create(a, rows, cols, d, marg, &po, &p);
-    if (st != LD_OK) return st;
-    uint64_t lo = 0, hi = 0;
-    ld_plan_range(p, &lo, &hi);
-    if (pieces > 1 && lo != ck.covered) {
-      ld_plan_destroy(p);
-      return ld_fail(LD_ERR_ARG, "piece %d starts at Gray index %llu, the checkpoint covers [0, %llu): the solve's "
-                     "geometry changed (options or device)", ck.next, (unsigned long long)lo, ck.covered);
-    }
-    ld_result r;
-    st = ld_plan_launch(p);
-    if (st == LD_OK) st = ld_plan_result(p, &r, nullptr);
-    ld_plan_destroy(p);
-    if (st != LD_OK) return st;
-    if (r.value > ck.value || (r.value == ck.value && r.gray_index < ck.index)) {
-      ck.value = r.value;
-      ck.index = r.gray_index;
-    }
-    ck.covered = hi;
-    ck.labelings += r.labelings;
-    ck.evaluated += r.evaluated;
-    ck.kernel_ms += r.kernel_ms;
-    kind = r.kernel_kind;
-    lane_bits = r.lane_bits;
-    ++ck.next;
-    ++ran;
-    if (!checkpoint_write(checkpoint_path, ck)) return ld_fail(LD_ERR_IO, "cannot write %s", checkpoint_path);
-  }
-  *done = ck.next == pieces ? 1 : 0;
-  memset(res, 0, sizeof *res);
-  res->value = ck.value;
-  res->gray_index = ck.index;
-  res->labelings = ck.labelings;
-  res->evaluated = ck.evaluated;
-  res->kernel_ms = (float)ck.kernel_ms;
-  res->kernel_kind = kind;
-  res->lane_bits = lane_bits;
-  if (*done && strategy) ld_gray_labels(ck.index, rows, d, strategy);
-  return LD_OK;
-}
-
-// ---------------------------------------------------------------------------
-// Pruned exact search (prune_kernel.cuh).  Exactly the plain enumeration's
-// result; the incumbent only decides how much is skipped.
-#include "../kernels/prune_kernel.cuh"
-
-namespace {
-
-// value of one labeling (labels of rows 0..R-2), int64
-long long labeling_value(const int64_t* a, int R, int C, int d, int marginal, const int32_t* lab) {
-  const int nm = d == 1 ? 1 : d;
-  std::vector<long long> s((size_t)nm * C, 0);
-  for (int l = 0; l < C; ++l) s[l] = a[(size_t)(R - 1) * C + l];
-  for (int i = 0; i < R - 1; ++i)
-    for (int l = 0; l < C; ++l) {
-      const long long x = a[(size_t)i * C + l];
-      if (d == 1) s[l] += lab[i] ? x : -x;
-      else s[(size_t)lab[i] * C + l] += x;
-    }
-  long long v = 0;
-  for (int m = 0; m < nm; ++m)
-    for (int l = 0; l < C; ++l) {
-      const long long x = s[(size_t)m * C + l];
-      v += (d == 1 && marginal && l == 0) ? x : (x < 0 ? -x : x);
-    }
-  return v;
-}
-
-// The norm of rows [0, r) alone (every labeling of them), for the bounds:
-// the plain solver on those rows plus a zero fixed row.  Falls back to the
-// always-valid sum of absolute entries when the submatrix is too large to
-// enumerate quickly.
-ld_status rest_norm(const int64_t* a, int C, int d, int marginal, int r, int device, long long* out) {
-  if (r <= 0) { *out = 0; return LD_OK; }
-  const int base = d <= 2 ? 2 : d;
-  if ((double)r * std::log2((double)base) > 34.0) {
-    long long s = 0;
-    for (int i = 0; i < r; ++i)
-      for (int l = 0; l < C; ++l) { const int64_t x = a[(size_t)i * C + l]; s += x < 0 ? -x : x; }
-    *out = s;
-    return LD_OK;
-  }
-  std::vector<int64_t> sub((size_t)(r + 1) * C, 0);
-  memcpy(sub.data(), a, sizeof(int64_t) * (size_t)r * C);
-  ld_options o;
-  ld_options_init(&o);
-  o.device = device;
-  ld_result res;
-  ld_status st = ld_solve_reduced(sub.data(), r + 1, C, d, marginal, &o, &res, nullptr);
-  if (st != LD_OK) return st;
-  *out = res.value;
-  return LD_OK;
-}
-
-}  // namespace
-
-extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int32_t d, int32_t marginal,
-                                     const ld_options* opt, const int32_t* incumbent_labels,
-                                     ld_result* res, int32_t* strategy, ld_prune_stats* stats) {
-  if (!a || !res || R < 1 || C < 1) return ld_fail(LD_ERR_ARG, "bad arguments");
-  ld_options o;
-  if (opt) o = *opt; else ld_options_init(&o);
-  ld_prune_stats ps;
-  memset(&ps, 0, sizeof ps);
-  ps.incumbent = LLONG_MIN;
-  if (incumbent_labels && R > 1) {
-    for (int i = 0; i < R - 1; ++i)
-      if (incumbent_labels[i] < 0 || incumbent_labels[i] >= (d == 1 ? 2 : d))
-        return ld_fail(LD_ERR_ARG, "incumbent label %d of row %d out of range", incumbent_labels[i], i);
-    ps.incumbent = labeling_value(a, R, C, d, marginal, incumbent_labels);
-  }
-  auto plain = [&]() -> ld_status {
-    ld_status s = ld_solve_reduced(a, R, C, d, marginal, &o, res, strategy);
-    ps.pruned = 0;
-    if (stats) *stats = ps;
-    return s;
-  };
-  if (d > 3 || R < 3 || C > LD_MAX_COLS || R > ld_max_rows_for(d)) return plain();
-  DeviceInfo di;
-  ld_status st = device_info(o.device, &di);
-  if (st != LD_OK) return st;
-  const Bounds bnd = compute_bounds(a, R, C, marginal);
-  if (bnd.overflow || bnd.total + (marginal ? bnd.K : 0) > (long long)INT32_MAX) return plain();
-
-  // table configuration with a pruned-kernel instance: the largest k whose
-  // table fits 48 KB
-  const int base = d <= 2 ? 2 : d, F = R - 1;
-  Choice ch;
-  const void* kb = nullptr;
-  const void* ks = nullptr;
-  int k = -1;
-  for (int kk = std::min(F - 1, 10); kk >= 0 && k < 0; --kk) {
-    const unsigned long long B = ipow(base, kk);
-    if (B > 1024) continue;
-    Choice c;
-    if (!table_config(a, R, C, d, marginal, kk, 0, &c)) continue;
-    // round to an instantiated shape
-    if (d == 1 && !(c.WB <= 2 && c.WA <= 16)) {
-      if (C > 64) continue;
-      c.order.clear();
-      for (int l = 0; l < C; ++l) c.order.push_back(l);
-      c.WB = round4(C); c.WA = 0; c.lane_bits = 32;
-    } else if (d >= 2) {
-      if (c.WA > 0) c.WA = round4(c.WA); else c.WB = round4(c.WB);
-    }
-    c.WT = round4(c.WB + c.WA);
-    const void* b1; const void* b2;
-    ld::prune_kernel_ptrs(d, c.WB, c.WA, &b1, &b2);
-    if (!b1 || B * (unsigned long long)(d * c.WT) * 4ull > 48ull * 1024ull) continue;
-    ch = c; kb = b1; ks = b2; k = kk;
-  }
-  if (k < 0) return plain();
-  const int nh = F - k;
-  // walk rows: every walk gets one bound in the first launch, so at most
-  // about 2^21 walks; the surviving walks' high indices are split over the
-  // threads of the scan, so long walks cost nothing extra there
-  int fw = std::min(nh, 5);
-  while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 21.0) ++fw;
-  const unsigned long long walk_len = ipow(base, fw), walks = ipow(base, nh - fw);
-  const int B = (int)ipow(base, k);
-  ps.low_rows = k; ps.walk_rows = fw;
-  ps.walks_total = walks;
-  ps.highs_total = walks * walk_len;
-  ps.block = (uint64_t)B;
-
-  // bounds of the rest rows, in the kernel's representation
-  long long m_low = 0, m_walk = 0, kl = 0, kh = 0;
-  st = rest_norm(a, C, d, marginal, k, o.device, &m_low);
-  if (st == LD_OK) st = rest_norm(a, C, d, marginal, k + fw, o.device, &m_walk);
-  if (st != LD_OK) return st;
-  if (d == 1 && marginal) {
-    for (int i = 0; i < R; ++i) { const int64_t v = a[(size_t)i * C]; (i < k ? kl : kh) += v < 0 ? -v : v; }
-    m_low += kl;
-    m_walk += kl;
-  }
-  const long long offset = kh + kl;
-  const long long thr = ps.incumbent == LLONG_MIN ? LLONG_MIN : ps.incumbent + offset;
-
-  // image: header | tot | h0 | tb | ttop | thigh | rows
-  const int WT = ch.WT;
-  std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0), ttop(C, 0), thigh(C, 0);
-  for (int i = 0; i < R; ++i)
-    for (int l = 0; l < C; ++l) {
-      const int64_t x = a[(size_t)i * C + l];
-      tot[l] += x;
-      if (i >= k) thigh[l] += x;
-      if (i >= k + fw) ttop[l] += x;
-    }
-  if (d == 1) {
-    for (int l = 0; l < C; ++l) h0[l] = a[(size_t)(R - 1) * C + l];
-    if (marginal) { h0[0] += kh; tb[0] = -kl; }
-  }
-  const size_t offTot = 256, offH0 = 512, offTb = 768, offTtop = 1024, offThigh = 1280, offA = 1536;
-  const size_t upload = offA + (size_t)R * WT * 4;
-  std::vector<char> image(upload, 0);
-  const long long gmin = LLONG_MIN;
-  memcpy(image.data() + 8, &gmin, sizeof gmin);
-  pack_row(tot.data(), ch, (uint32_t*)(image.data() + offTot));
-  pack_row(h0.data(), ch, (uint32_t*)(image.data() + offH0));
-  pack_row(tb.data(), ch, (uint32_t*)(image.data() + offTb));
-  pack_row(ttop.data(), ch, (uint32_t*)(image.data() + offTtop));
-  pack_row(thigh.data(), ch, (uint32_t*)(image.data() + offThigh));
-  for (int i = 0; i < R; ++i) pack_row(a + (size_t)i * C, ch, (uint32_t*)(image.data() + offA) + (size_t)i * WT);
-
-  const size_t smem_b = (size_t)ld::prune_smem_words(d, WT, R, B, false) * 4;
-  const size_t smem_s = (size_t)ld::prune_smem_words(d, WT, R, B, true) * 4;
-  int bps_b = 0, bps_s = 0;
-  if (cudaSetDevice(o.device) != cudaSuccess ||
-      ld_raise_smem_limit(kb, smem_b) != cudaSuccess || ld_raise_smem_limit(ks, smem_s) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, kb, ld::kPruneThreads, smem_b) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_s, ks, ld::kPruneThreads, smem_s) != cudaSuccess ||
-      bps_b < 1 || bps_s < 1)
-    return ld_fail(LD_ERR_CUDA, "pruned kernels do not fit an SM");
-  const unsigned long long blocks_b = std::max(1ull, std::min<unsigned long long>((unsigned long long)di.sms * bps_b,
-                                                   (walks + ld::kPruneThreads - 1) / ld::kPruneThreads));
-  const unsigned long long blocks_s = (unsigned long long)di.sms * bps_s;
-  const size_t off_slots = align256(upload);
-  const size_t off_list = off_slots + align256(blocks_s * sizeof(ld::Slot));
-  const size_t off_cnt = off_list + align256(walks * 8);
-  const size_t dbytes = off_cnt + 256;
-  if (o.device < 0 || o.device >= 64) return ld_fail(LD_ERR_ARG, "device %d out of range", o.device);
-  std::lock_guard<std::mutex> lock(g_pws_mu[o.device]);
-  Resources* r = &g_pws[o.device];
-  // the workspace keeps the stream it was created with: the caller's, or its own
-  if (r->device >= 0 && (cudaStream_t)o.stream != (r->own_stream ? nullptr : r->stream)) resources_release(r);
-  st = resources_acquire(r, o.device, (cudaStream_t)o.stream, dbytes, 256);
-  if (st != LD_OK) return st;
-  char* dmem = (char*)r->dmem;
-  cudaStream_t s = r->stream;
-  ld::Slot* out_h = (ld::Slot*)r->hstage;
-  unsigned long long* hstat = (unsigned long long*)((char*)r->hstage + 64);
-  float ms_b = 0.f, ms_s = 0.f;
-  auto fail = [&](const char* what, cudaError_t e) {
-    cudaStreamSynchronize(s);
-    return ld_fail(LD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
-  };
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(dmem + off_cnt, 0, 256, s)) != cudaSuccess) return fail("memset", e);
-  if ((e = cudaMemcpyAsync(dmem, image.data(), upload, cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload", e);
-  {
-    ld::PruneArgs args;
-    ld::TableArgs& t = args.t;
-    t.A = (const uint32_t*)(dmem + offA);
-    t.tot = (const uint32_t*)(dmem + offTot);
-    t.hinit = (const uint32_t*)(dmem + offH0);
-    t.tbias = (const uint32_t*)(dmem + offTb);
-    t.R = R; t.k = k; t.B = B; t.fw = fw;
-    t.walk_len = walk_len; t.walk_begin = 0; t.walk_end = walks;
-    // d = 3: the walk bound also drops walks that hold no class minimum
-    t.sym_digits = (d == 3 && !o.enumerate_all && nh - fw > 0) ? nh - fw : 0;
-    t.sym_table = nullptr; t.rank_begin = t.rank_end = 0;
-    t.value_offset = offset;
-    t.red.counter = (unsigned int*)(dmem + 0);
-    t.red.gvalue = (long long*)(dmem + 8);
-    t.red.result = (ld::Slot*)(dmem + 16);
-    t.red.slots = (ld::Slot*)(dmem + off_slots);
-    args.ttop = (const uint32_t*)(dmem + offTtop);
-    args.thigh = (const uint32_t*)(dmem + offThigh);
-    args.threshold = thr;
-    args.m_walk = m_walk;
-    args.m_low = m_low;
-    args.list = (unsigned long long*)(dmem + off_list);
-    args.list_count = (unsigned long long*)(dmem + off_cnt);
-    args.stats = (unsigned long long*)(dmem + off_cnt + 8);
-    void* params[] = {&args};
-    if ((e = cudaEventRecord(r->ev0, s)) != cudaSuccess) return fail("event", e);
-    if ((e = cudaLaunchKernel(kb, dim3((unsigned)blocks_b), dim3(ld::kPruneThreads), params, smem_b, s)) != cudaSuccess)
-      return fail("walk bound launch", e);
-    if ((e = cudaEventRecord(r->ev1, s)) != cudaSuccess) return fail("event", e);
-    // When more than a quarter of the walks survive their bound the scan
-    // would do most of the plain enumeration's work at a lower rate: run the
-    // plain enumeration instead (same result).
-    if ((e = cudaMemcpyAsync(hstat, dmem + off_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) !=
-        cudaSuccess)
-      return fail("survivors", e);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail("walk bound", e);
-    if (o.prune_policy == 0 && hstat[0] * 4ull > walks) {
-      cudaEventElapsedTime(&ms_b, r->ev0, r->ev1);
-      ps.walks_kept = hstat[0];
-      ps.bound_ms = ms_b;
-      return plain();
-    }
-    if ((e = cudaLaunchKernel(ks, dim3((unsigned)blocks_s), dim3(ld::kPruneThreads), params, smem_s, s)) != cudaSuccess)
-      return fail("scan launch", e);
-    if ((e = cudaEventRecord(r->ev2, s)) != cudaSuccess) return fail("event", e);
-  }
-  if ((e = cudaMemcpyAsync(out_h, dmem + 16, sizeof(ld::Slot), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-    return fail("result", e);
-  if ((e = cudaMemcpyAsync(hstat, dmem + off_cnt, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-    return fail("stats", e);
-  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail("solve", e);
-  cudaEventElapsedTime(&ms_b, r->ev0, r->ev1);
-  cudaEventElapsedTime(&ms_s, r->ev1, r->ev2);
-  const ld::Slot out = *out_h;
-  if (ps.incumbent != LLONG_MIN && out.value < ps.incumbent)
-    return ld_fail(LD_ERR_CUDA, "internal: pruned result %lld below the incumbent %lld", (long long)out.value,
-                   (long long)ps.incumbent);
-  memset(res, 0, sizeof *res);
-  res->value = out.value;
-  res->gray_index = out.index;
-  res->labelings = ld_labelings(R, d);
-  res->kernel_ms = ms_b + ms_s;
-  res->kernel_kind = LD_KERNEL_TABLE;
-  res->lane_bits = ch.lane_bits;
-  res->h2d_bytes = upload;
-  res->d2h_bytes = sizeof out + 4 * sizeof(unsigned long long);
-  res->evaluated = hstat[2] * (unsigned long long)B;   // high indices whose block was scanned
-  if (strategy) ld_gray_labels(out.index, R, d, strategy);
-  ps.pruned = 1;
-  ps.walks_kept = hstat[1];
-  ps.highs_kept = hstat[2];
-  ps.highs_visited = hstat[3];
-  ps.bound_ms = ms_b;
-  ps.scan_ms = ms_s;
-  if (stats) *stats = ps;
-  return LD_OK;
-}
-
-// ---------------------------------------------------------------------------
-// Batched solves: one persistent kernel per lane class pulling (matrix, walk
-// range) chunks from a device queue (batch_kernel.cuh); the class kernels
-// run concurrently on forked streams; everything is captured once into a
-// CUDA graph that each ld_batch_launch replays.  Matrices outside the batch
-// lane classes (d >= 4, more columns, 64-bit sums) get their own plans,
-// launched inside the same graph.
-#include <map>
-#include <tuple>
-
-#include "../kernels/batch_kernel.cuh"
-
-namespace {
-
-struct BatchClass {
-  int D = 0, WB = 0, WA = 0;
-  const void* kfn = nullptr;
-  size_t smem = 0;
-  int bps = 1;
-  std::vector<int> probs;         // problem indices, largest first
-  int wpt = 1;                    // walks per thread per chunk
-  double grid_frac = 1.0;         // persistent CTAs per SM, as a fraction of the occupancy limit
-  const void* kfn_split = nullptr;  // column-split instance (wide int32 classes), or null
-  size_t smem_split = 0;
-  int bps_split = 0;
-  bool split = false;             // the autotuner chose the column-split instance
-  float tuned[2] = {0.f, 0.f};    // autotuner: best ms per 1e9 labelings, plain / split instance
-  const void* fn() const { return split ? kfn_split : kfn; }
-  size_t shm() const { return split ? smem_split : smem; }
-  int blocks_per_sm() const { return split ? bps_split : bps; }
-  int chunk_first = 0, nchunks = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
-};
-
-// autotuner cache: (D, WB, WA, log2 of the mean walks per problem, batch_split option)
-//   -> (wpt, grid fraction, split)
-std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool>> g_tune;
-
-}  // namespace
-
-struct ld_batch {
-  int n = 0, device = 0;
-  std::vector<int> R, C, d, marginal;
-  std::vector<unsigned long long> labelings;
-  std::vector<unsigned long long> evaluated;  // labelings the kernels compute a value for
-  std::vector<int> cls;                       // class index, or -1 (own plan), or -2 (nothing to do)
-  std::vector<ld_plan*> plans;                // per problem, or null
-  std::vector<BatchClass> classes;
-  std::vector<ld::BatchProblem> hprob;        // device pointers filled after allocation
-  std::vector<ld::BatchChunk> hchunks;
-  std::vector<int> range_first, range_end;
-  char* dmem = nullptr;
-  size_t off_prob = 0, off_chunks = 0, off_heads = 0, off_cres = 0, off_ranges = 0, off_res = 0;
-  ld::Slot* hres = nullptr;                   // pinned
-  cudaStream_t stream = nullptr;
-  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  bool launched = false;
-  std::string desc;
-};
-
-static void batch_free(ld_batch* b) {
-  if (!b) return;
-  cudaSetDevice(b->device);
-  if (b->stream) cudaStreamSynchronize(b->stream);
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->graph) cudaGraphDestroy(b->graph);
-  for (auto* p : b->plans) if (p) plan_free(p);
-  for (auto& c : b->classes) {
-    if (c.stream) cudaStreamDestroy(c.stream);
-    if (c.done) cudaEventDestroy(c.done);
-  }
-  if (b->dmem) cudaFree(b->dmem);
-  if (b->hres) cudaFreeHost(b->hres);
-  if (b->fork) cudaEventDestroy(b->fork);
-  if (b->ev0) cudaEventDestroy(b->ev0);
-  if (b->ev1) cudaEventDestroy(b->ev1);
-  if (b->stream) cudaStreamDestroy(b->stream);
-  delete b;
-}
-
-// chunks of one class for a given walks-per-thread; returns the number of chunks
-static int batch_chunks(const ld_batch* b, const BatchClass& c, int wpt,
-                        const std::vector<unsigned long long>& walks, std::vector<ld::BatchChunk>* out) {
-  const unsigned long long span = (unsigned long long)ld::kBatchThreads * (unsigned long long)wpt;
-  int n = 0;
-  for (int p : c.probs) {
-    for (unsigned long long w = 0; w < walks[p]; w += span) {
-      ld::BatchChunk ch;
-      ch.walk_begin = w;
-      ch.walk_end = std::min(walks[p], w + span);
-      ch.problem = p;
-      ch.pad = 0;
-      if (out) out->push_back(ch);
-      ++n;
-    }
-  }
-  (void)b;
-  return n;
-}
-
-extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, const int32_t* rows,
-                                     const int32_t* cols, const int32_t* ds, const int32_t* margs,
-                                     const ld_options* opt, int32_t autotune, ld_batch** out) {
-  if (!out || count < 1 || !mats || !rows || !cols || !ds) return ld_fail(LD_ERR_ARG, "bad batch arguments");
-  ld_options o;
-  if (opt) o = *opt; else ld_options_init(&o);
-  DeviceInfo di;
-  ld_status st = device_info(o.device, &di);
-  if (st != LD_OK) return st;
-  if (cudaSetDevice(o.device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "cudaSetDevice failed");
-  ld_batch* b = new ld_batch();
-  b->n = count;
-  b->device = o.device;
-  b->cls.assign(count, -2);
-  b->evaluated.assign(count, 0);
-  b->plans.assign(count, nullptr);
-  b->range_first.assign(count, 0);
-  b->range_end.assign(count, 0);
-  std::vector<unsigned long long> walks(count, 0);
-  std::vector<std::vector<char>> images(count);
-  std::map<std::tuple<int, int, int>, int> class_of;
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
-    batch_free(b);
-    return ld_fail(LD_ERR_CUDA, "stream/event creation failed");
-  }
-  for (int p = 0; p < count; ++p) {
-    const int R = rows[p], C = cols[p], d = ds[p], marg = margs ? margs[p] : 0;
-    const int64_t* a = mats[p];
-    b->R.push_back(R); b->C.push_back(C); b->d.push_back(d); b->marginal.push_back(marg);
-    if (!a || R < 1 || C < 1 || d < 1 || d > LD_MAX_D || (marg && d != 1) || C > LD_MAX_COLS ||
-        R > ld_max_rows_for(d) || ld_labelings(R, d) >= (1ull << 63)) {
-      batch_free(b);
-      return ld_fail(LD_ERR_ARG, "batch entry %d: invalid or too large (%d x %d, d=%d)", p, R, C, d);
-    }
-    b->labelings.push_back(ld_labelings(R, d));
-    const Bounds bnd = compute_bounds(a, R, C, marg);
-    const bool fits32 = !bnd.overflow && bnd.total + (marg ? bnd.K : 0) <= (long long)INT32_MAX &&
-                        std::max(bnd.colbound, marg ? 2 * bnd.K : 0LL) <= (long long)INT32_MAX;
-    // batch lane class: all columns int8 (WA a multiple of 4) or all int32 (WB a multiple of 8)
-    Choice ch;
-    int k = -1;
-    const int base = d <= 2 ? 2 : d, F = R - 1;
-    if (d <= 3 && fits32 && R >= 2) {
-      for (int kk = std::min(F, 10); kk >= 0; --kk) {
-        const unsigned long long B = ipow(base, kk);
-        if (B > 1024) continue;
-        Choice c;
-        if (!table_config(a, R, C, d, marg, kk, 0, &c)) continue;
-        c.order.clear();
-        for (int l = 0; l < C; ++l) c.order.push_back(l);
-        if (c.WB == 0) { c.WA = round4(c.WA); }
-        else {
-          c.WB = (C + 7) & ~7; c.WA = 0;
-          if (c.WB > 64) continue;
-          // with all-int32 lanes the column order is the identity and every column is wide
-        }
-        c.WT = round4(c.WB + c.WA);
-        if (!ld::batch_kernel_ptr(d, c.WB, c.WA) || B * (unsigned long long)(d * c.WT) > 4096ull) continue;
-        if (c.WB > 0) {      // re-pack every column as int32 (table_config may have put some in int8)
-          c.order.clear();
-          for (int l = 0; l < C; ++l) c.order.push_back(l);
-        } else {
-          // all narrow: table_config's order is identity-compatible
-        }
-        c.lane_bits = c.WB > 0 ? 32 : 8;
-        ch = c; k = kk;
-        break;
-      }
-    }
-    if (k < 0) {                       // own plan, captured in the same graph
-      ld_options po = o;
-      po.stream = b->stream;
-      po.shard_count = 1; po.shard_index = 0;
-      ld_plan* plan = nullptr;
-      st = plan_build(a, R, C, d, marg, &po, nullptr, &plan);
-      if (st != LD_OK) { batch_free(b); return st; }
-      b->plans[p] = plan;
-      b->cls[p] = -1;
-      b->evaluated[p] = plan_evaluated(plan);
-      continue;
-    }
-    const auto key = std::make_tuple(d, ch.WB, ch.WA);
-    auto it = class_of.find(key);
-    int ci;
-    if (it == class_of.end()) {
-      ci = (int)b->classes.size();
-      class_of[key] = ci;
-      BatchClass bc;
-      bc.D = d; bc.WB = ch.WB; bc.WA = ch.WA;
-      bc.kfn = ld::batch_kernel_ptr(d, ch.WB, ch.WA);
-      if (ch.WA == 0 && o.batch_split >= 0) bc.kfn_split = ld::batch_split_kernel_ptr(d, ch.WB);
-      b->classes.push_back(bc);
-    } else {
-      ci = it->second;
-    }
-    b->cls[p] = ci;
-    BatchClass& bc = b->classes[ci];
-    bc.probs.push_back(p);
-    const int nh = F - k;
-    // walks per matrix: at most 2^16 (enough chunks to spread one large matrix)
-    int fw = 0;
-    while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 16.0) ++fw;
-    walks[p] = ipow(base, nh - fw);
-    const int B = (int)ipow(base, k), WT = ch.WT;
-    bc.smem = std::max(bc.smem, (size_t)ld::table_smem_words(d, WT, R, B) * 4);
-    if (bc.kfn_split)
-      bc.smem_split = std::max(bc.smem_split, (size_t)ld::batch_split_smem_words(d, ch.WB, R, B) * 4);
-    // image: tot | h0 | tb | rows (each vector padded to 256 bytes)
-    std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
-    long long kl = 0, kh = 0;
-    for (int i = 0; i < R; ++i)
-      for (int l = 0; l < C; ++l) tot[l] += a[(size_t)i * C + l];
-    if (d == 1) {
-      for (int l = 0; l < C; ++l) h0[l] = a[(size_t)(R - 1) * C + l];
-      if (marg) {
-        for (int i = 0; i < R; ++i) { const int64_t v = a[(size_t)i * C]; (i < k ? kl : kh) += v < 0 ? -v : v; }
-        h0[0] += kh; tb[0] = -kl;
-      }
-    }
-    std::vector<char>& img = images[p];
-    img.assign(768 + align256((size_t)R * WT * 4), 0);
-    pack_row(tot.data(), ch, (uint32_t*)(img.data() + 0));
-    pack_row(h0.data(), ch, (uint32_t*)(img.data() + 256));
-    pack_row(tb.data(), ch, (uint32_t*)(img.data() + 512));
-    for (int i = 0; i < R; ++i) pack_row(a + (size_t)i * C, ch, (uint32_t*)(img.data() + 768) + (size_t)i * WT);
-    ld::BatchProblem bp{};
-    bp.R = R; bp.k = k; bp.B = B; bp.fw = fw;
-    bp.walk_len = ipow(base, fw);
-    bp.sym_pw = 1;
-    uint64_t run = walks[p];
-    if (d == 3 && !o.enumerate_all && nh - fw > 0 &&
-        ld_symmetry_walks(d, nh - fw, 0, walks[p], &run) == LD_OK) {
-      bp.sym_digits = nh - fw;
-      bp.sym_pw = ipow(base, nh - fw - 1);
-    } else {
-      run = walks[p];
-    }
-    b->evaluated[p] = (unsigned long long)run * bp.walk_len * (unsigned long long)B;
-    bp.value_offset = kh + kl;
-    b->hprob.resize(count);
-    b->hprob[p] = bp;
-  }
-  b->hprob.resize(count);
-  // classes: largest matrices first, occupancy, streams
-  for (auto& c : b->classes) {
-    std::stable_sort(c.probs.begin(), c.probs.end(),
-                     [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
-    if (ld_raise_smem_limit(c.kfn, c.smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps, c.kfn, ld::kBatchThreads, c.smem) != cudaSuccess ||
-        c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
-      batch_free(b);
-      return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d WA=%d does not fit an SM", c.D, c.WB, c.WA);
-    }
-    if (c.kfn_split && (ld_raise_smem_limit(c.kfn_split, c.smem_split) != cudaSuccess ||
-                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps_split, c.kfn_split, ld::kBatchThreads,
-                                                                      c.smem_split) != cudaSuccess ||
-                        c.bps_split < 1)) {
-      cudaGetLastError();
-      c.kfn_split = nullptr;
-    }
-  }
-  // device memory: images, problem table, chunks (sized for the largest wpt
-  // candidate = the fewest chunks is wpt 8; the most is wpt 1), heads,
-  // chunk results, ranges, results
-  size_t bytes = 0;
-  std::vector<size_t> img_off(count, 0);
-  for (int p = 0; p < count; ++p)
-    if (b->cls[p] >= 0) { img_off[p] = bytes; bytes += align256(images[p].size()); }
-  int max_chunks = 0;
-  for (auto& c : b->classes) max_chunks += batch_chunks(b, c, 1, walks, nullptr);
-  b->off_prob = bytes;   bytes += align256(sizeof(ld::BatchProblem) * count);
-  b->off_chunks = bytes; bytes += align256(sizeof(ld::BatchChunk) * std::max(1, max_chunks));
-  b->off_heads = bytes;  bytes += align256(sizeof(unsigned int) * std::max<size_t>(1, b->classes.size()));
-  b->off_cres = bytes;   bytes += align256(sizeof(ld::Slot) * std::max(1, max_chunks));
-  b->off_ranges = bytes; bytes += align256(sizeof(int) * 2 * (size_t)count);
-  b->off_res = bytes;    bytes += align256(sizeof(ld::Slot) * count);
-  if (cudaMalloc(&b->dmem, bytes) != cudaSuccess || cudaMallocHost((void**)&b->hres, sizeof(ld::Slot) * count) != cudaSuccess) {
-    batch_free(b);
-    return ld_fail(LD_ERR_CUDA, "batch allocation of %zu bytes failed", bytes);
-  }
-  std::vector<char> hostimg(b->off_prob, 0);
-  for (int p = 0; p < count; ++p) {
-    if (b->cls[p] < 0) continue;
-    memcpy(hostimg.data() + img_off[p], images[p].data(), images[p].size());
-    const char* base_ptr = b->dmem + img_off[p];
-    b->hprob[p].tot = (const uint32_t*)(base_ptr + 0);
-    b->hprob[p].hinit = (const uint32_t*)(base_ptr + 256);
-    b->hprob[p].tbias = (const uint32_t*)(base_ptr + 512);
-    b->hprob[p].A = (const uint32_t*)(base_ptr + 768);
-  }
-  if (cudaMemcpy(b->dmem, hostimg.data(), hostimg.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(b->dmem + b->off_prob, b->hprob.data(), sizeof(ld::BatchProblem) * count, cudaMemcpyHostToDevice) != cudaSuccess) {
-    batch_free(b);
-    return ld_fail(LD_ERR_CUDA, "batch upload failed");
-  }
-
-  auto build_queue = [&]() -> ld_status {
-    b->hchunks.clear();
-    for (auto& c : b->classes) {
-      c.chunk_first = (int)b->hchunks.size();
-      c.nchunks = batch_chunks(b, c, c.wpt, walks, &b->hchunks);
-    }
-    for (int p = 0; p < count; ++p) { b->range_first[p] = 0; b->range_end[p] = 0; }
-    for (size_t i = 0; i < b->hchunks.size(); ++i) {
-      const int p = b->hchunks[i].problem;
-      if (b->range_end[p] == 0) b->range_first[p] = (int)i;
-      b->range_end[p] = (int)i + 1;
-    }
-    std::vector<int> ranges(2 * (size_t)count);
-    for (int p = 0; p < count; ++p) { ranges[2 * p] = b->range_first[p]; ranges[2 * p + 1] = b->range_end[p]; }
-    if (!b->hchunks.empty() &&
-        cudaMemcpy(b->dmem + b->off_chunks, b->hchunks.data(), sizeof(ld::BatchChunk) * b->hchunks.size(),
-                   cudaMemcpyHostToDevice) != cudaSuccess)
-      return ld_fail(LD_ERR_CUDA, "chunk upload failed");
-    if (cudaMemcpy(b->dmem + b->off_ranges, ranges.data(), sizeof(int) * ranges.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-      return ld_fail(LD_ERR_CUDA, "range upload failed");
-    return LD_OK;
-  };
-  auto class_args = [&](const BatchClass& c) {
-    ld::BatchArgs args;
-    args.problems = (const ld::BatchProblem*)(b->dmem + b->off_prob);
-    args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks) + c.chunk_first;
-    args.nchunks = c.nchunks;
-    args.head = (unsigned int*)(b->dmem + b->off_heads) + (&c - b->classes.data());
-    args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres) + c.chunk_first;
-    return args;
-  };
-  auto class_grid = [&](const BatchClass& c) {
-    const int g = (int)std::max(1.0, std::floor((double)di.sms * c.blocks_per_sm() * c.grid_frac));
-    return std::min(g, std::max(1, c.nchunks));
-  };
-
-  // autotuner: walks per thread per chunk and the persistent grid size, timed
-  // on one wave of each class's chunks from its median matrix on; cached per
-  // class shape and matrix size.
-  for (auto& c : b->classes) {
-    double mean = 0;
-    for (int p : c.probs) mean += (double)walks[p];
-    mean /= std::max<size_t>(1, c.probs.size());
-    const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)), (int)o.batch_split);
-    {
-      std::lock_guard<std::mutex> lk(g_tune_mu);
-      auto it = g_tune.find(key);
-      if (it != g_tune.end()) {
-        std::tie(c.wpt, c.grid_frac, c.split) = it->second;
-        if (!c.kfn_split) c.split = false;
-        if (o.batch_split > 0 && c.kfn_split) c.split = true;
-        continue;
-      }
-    }
-    if (o.batch_split > 0 && c.kfn_split) c.split = true;
-    if (!autotune) continue;
-    float best_ms = 1e30f;
-    int best_wpt = 1;
-    double best_frac = 1.0;
-    bool best_split = false;
-    for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
-    for (int wpt : {1, 2, 4, 8}) {
-      for (double frac : {0.5, 1.0}) {   // persistent CTAs: half or all of the occupancy limit
-        std::vector<ld::BatchChunk> all;
-        batch_chunks(b, c, wpt, walks, &all);
-        // one wave of chunks (a chunk per resident CTA), starting at the
-        // class's median matrix: the class's steady state at a fraction of
-        // the cost of its largest matrices
-        const int wave = di.sms * (variant ? c.bps_split : c.bps);
-        size_t first = 0;
-        const int median = c.probs[c.probs.size() / 2];
-        while (first < all.size() && all[first].problem != median) ++first;
-        if (first + (size_t)wave > all.size()) first = all.size() > (size_t)wave ? all.size() - wave : 0;
-        std::vector<ld::BatchChunk> chunks(all.begin() + first, all.end());
-        const int sample = std::min<int>((int)chunks.size(), wave);
-        if (sample < 1) continue;
-        cudaMemcpy(b->dmem + b->off_chunks, chunks.data(), sizeof(ld::BatchChunk) * sample, cudaMemcpyHostToDevice);
-        BatchClass tc = c;
-        tc.chunk_first = 0; tc.nchunks = sample; tc.grid_frac = frac; tc.split = variant == 1;
-        ld::BatchArgs args = class_args(c);
-        args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks);
-        args.nchunks = sample;
-        args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres);
-        float ms = 0;
-        for (int rep = 0; rep < 1; ++rep) {
-          cudaMemsetAsync(args.head, 0, sizeof(unsigned int), b->stream);
-          cudaEventRecord(b->ev0, b->stream);
-          void* params[] = {&args};
-          cudaLaunchKernel(tc.fn(), dim3(class_grid(tc)), dim3(ld::kBatchThreads), params, tc.shm(), b->stream);
-          cudaEventRecord(b->ev1, b->stream);
-          cudaEventSynchronize(b->ev1);
-          cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-        }
-        // normalize by the labelings the sample covered
-        double lab = 0;
-        for (int i = 0; i < sample; ++i)
-          lab += (double)(chunks[i].walk_end - chunks[i].walk_begin) * (double)b->hprob[chunks[i].problem].walk_len *
-                 (double)b->hprob[chunks[i].problem].B;
-        const float per = (float)(ms / std::max(1.0, lab));
-        if (per < best_ms) { best_ms = per; best_wpt = wpt; best_frac = frac; best_split = variant == 1; }
-        if (c.tuned[variant] == 0.f || per * 1e9f < c.tuned[variant]) c.tuned[variant] = per * 1e9f;
-      }
-    }
-    if (cudaGetLastError() != cudaSuccess) { batch_free(b); return ld_fail(LD_ERR_CUDA, "autotune launch failed"); }
-    c.wpt = best_wpt; c.grid_frac = best_frac; c.split = best_split;
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[key] = std::make_tuple(best_wpt, best_frac, best_split);
-  }
-  st = build_queue();
-  if (st != LD_OK) { batch_free(b); return st; }
-
-  // capture the whole batch solve into one graph
-  cudaStream_t s = b->stream;
-  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) e = cudaMemsetAsync(b->dmem + b->off_heads, 0, sizeof(unsigned int) * std::max<size_t>(1, b->classes.size()), s);
-  if (e == cudaSuccess) e = cudaEventRecord(b->fork, s);
-  for (auto& c : b->classes) {
-    if (e != cudaSuccess) break;
-    e = cudaStreamWaitEvent(c.stream, b->fork, 0);
-    ld::BatchArgs args = class_args(c);
-    void* params[] = {&args};
-    if (e == cudaSuccess && c.nchunks > 0)
-      e = cudaLaunchKernel(c.fn(), dim3(class_grid(c)), dim3(ld::kBatchThreads), params, c.shm(), c.stream);
-    if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
-  }
-  ld_status pst = LD_OK;
-  for (int p = 0; p < count && e == cudaSuccess && pst == LD_OK; ++p)
-    if (b->plans[p]) pst = plan_enqueue(b->plans[p]);
-  for (auto& c : b->classes) if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c.done, 0);
-  if (e == cudaSuccess) {
-    const ld::Slot* cres = (const ld::Slot*)(b->dmem + b->off_cres);
-    const int* ranges = (const int*)(b->dmem + b->off_ranges);
-    ld::Slot* res = (ld::Slot*)(b->dmem + b->off_res);
-    int n = count;
-    void* params[] = {(void*)&cres, (void*)&ranges, (void*)&n, (void*)&res};
-    e = cudaLaunchKernel(ld::batch_fold_kernel_ptr(), dim3((count + 127) / 128), dim3(128), params, 0, s);
-  }
-  for (int p = 0; p < count && e == cudaSuccess; ++p)
-    if (b->plans[p])
-      e = cudaMemcpyAsync(b->dmem + b->off_res + sizeof(ld::Slot) * p, b->plans[p]->red.result, sizeof(ld::Slot),
-                          cudaMemcpyDeviceToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(b->hres, b->dmem + b->off_res, sizeof(ld::Slot) * count, cudaMemcpyDeviceToHost, s);
-  cudaGraph_t g = nullptr;
-  cudaError_t e2 = cudaStreamEndCapture(s, &g);
-  if (e == cudaSuccess) e = e2;
-  b->graph = g;
-  if (e == cudaSuccess && pst == LD_OK) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-  if (e != cudaSuccess || pst != LD_OK) {
-    batch_free(b);
-    return pst != LD_OK ? pst : ld_fail(LD_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
-  }
-  char buf[256];
-  snprintf(buf, sizeof buf, "%d matrices: %zu classes, %zu chunks, %d own plans", count, b->classes.size(),
-           b->hchunks.size(), (int)std::count_if(b->plans.begin(), b->plans.end(), [](ld_plan* q) { return q != nullptr; }));
-  b->desc = buf;
-  for (auto& c : b->classes) {
-    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, grid=%d%s", c.D, c.WB, c.WA,
-             c.probs.size(), c.nchunks, c.wpt, class_grid(c), c.split ? ", column split" : "");
-    b->desc += buf;
-    if (c.tuned[0] > 0.f && c.tuned[1] > 0.f) {
-      snprintf(buf, sizeof buf, " (tuned ms per 1e9 labelings: %.3f, split %.3f)", c.tuned[0], c.tuned[1]);
-      b->desc += buf;
-    }
-  }
-  *out = b;
-  return LD_OK;
-}
-
-extern "C" ld_status ld_batch_launch(ld_batch* b) {
-  if (!b || !b->exec) return ld_fail(LD_ERR_ARG, "null batch");
-  LD_CUDA(cudaSetDevice(b->device));
-  // timing events outside the graph (events recorded during capture cannot be timed)
-  LD_CUDA(cudaEventRecord(b->ev0, b->stream));
-  LD_CUDA(cudaGraphLaunch(b->exec, b->stream));
-  LD_CUDA(cudaEventRecord(b->ev1, b->stream));
-  b->launched = true;
-  return LD_OK;
-}
-
-extern "C" ld_status ld_batch_results(ld_batch* b, int64_t* values, uint64_t* gray_indices, float* ms) {
-  if (!b || !values) return ld_fail(LD_ERR_ARG, "null argument");
-  if (!b->launched) return ld_fail(LD_ERR_ARG, "batch has not been launched");
-  LD_CUDA(cudaSetDevice(b->device));
-  LD_CUDA(cudaStreamSynchronize(b->stream));
-  for (int p = 0; p < b->n; ++p) {
-    values[p] = b->hres[p].value;
-    if (gray_indices) gray_indices[p] = b->hres[p].index;
-  }
-  if (ms) {
-    float t = 0.f;
-    LD_CUDA(cudaEventElapsedTime(&t, b->ev0, b->ev1));
-    *ms = t;
-  }
-  return LD_OK;
-}
-
-extern "C" ld_status ld_batch_describe(const ld_batch* b, char* buf, size_t cap) {
-  if (!b || !buf) return ld_fail(LD_ERR_ARG, "null argument");
-  snprintf(buf, cap, "%s", b->desc.c_str());
-  return LD_OK;
-}
-
-extern "C" ld_status ld_batch_evaluated(const ld_batch* b, uint64_t* evaluated) {
-  if (!b || !evaluated) return ld_fail(LD_ERR_ARG, "null argument");
-  for (int p = 0; p < b->n; ++p) evaluated[p] = b->evaluated[p];
-  return LD_OK;
-}
-
-extern "C" void ld_batch_destroy(ld_batch* b) { batch_free(b); }
