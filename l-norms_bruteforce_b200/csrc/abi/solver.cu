@@ -342,11 +342,13 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
       if (sym && nh - f > 0 && ld_symmetry_walks(d, nh - f, lo, hi, &c) != LD_OK) c = hi - lo;
       return (unsigned long long)c;
     };
-    // walk length: as long as the walks still number >= 32 per thread of a
+    // walk length: as long as the walks still number >= 16 per thread of a
     // full grid (d <= 2), or >= 4 (d >= 3, whose walk seeding costs 64-bit
-    // divisions per high digit: longer walks measured 9 % faster on 20x30
-    // d = 3)
-    const unsigned long long per_thread = D >= 3 ? 4ull : 32ull;
+    // divisions per high digit).  Longer walks seed less often; the kernel is
+    // issue-bound, so warps left with one walk more than others finish
+    // faster as the rest drain.  Measured: 20x30 d = 3 9 % faster at 4 than
+    // at 32; 34x37 LM 3 % faster at 16 than at 32, 12 % slower at 8.
+    const unsigned long long per_thread = D >= 3 ? 4ull : 16ull;
     int fw = 0;
     while (fw < nh && walks_run(fw + 1, 0, ipow(base, nh - fw - 1)) >= per_thread * full) ++fw;
     if (o.tile > 0) fw = std::min(nh, o.tile);
