@@ -103,6 +103,8 @@ struct ld_plan {
   ldsolve::Choice ch;
   ldsolve::Bounds bounds{};
   int k = 0, B = 1, fw = 0;                       // table geometry
+  // walks: the table kernel's blocks of high indices, or (wide kernel with
+  // label symmetry) runs of walk_len consecutive indices
   unsigned long long walk_len = 1, walks = 1, walk_begin = 0, walk_end = 1;
   int sym_digits = 0;                             // label symmetry: walk-number digits
   size_t sym_off = 0;                             // completion counts in the device image
