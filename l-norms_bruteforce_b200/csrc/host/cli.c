@@ -126,8 +126,9 @@ int ld_cli_main(int argc, char **argv) {
     }
     const char *verbose = getenv("LD_VERBOSE");
     if (verbose && verbose[0] == '1')
-        fprintf(stderr, "L_CUDA: kernel %d, %d-bit lanes, %llu labelings, %.3f ms\n", res.kernel_kind,
-                res.lane_bits, (unsigned long long)res.labelings, (double)res.kernel_ms);
+        fprintf(stderr, "L_CUDA: kernel %d, %d-bit lanes, %llu labelings (%llu evaluated), %.3f ms\n",
+                res.kernel_kind, res.lane_bits, (unsigned long long)res.labelings,
+                (unsigned long long)res.evaluated, (double)res.kernel_ms);
     free(strategy);
     ld_problem_destroy(p);
     return st == LD_OK ? 0 : 1;
