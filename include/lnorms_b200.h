@@ -348,6 +348,15 @@ ld_status ld_symmetry_walks(int32_t d, int32_t prefix_digits, uint64_t lo, uint6
 ld_status ld_symmetry_walk_at(int32_t d, int32_t prefix_digits, uint64_t rank, uint64_t *w);
 
 /* ---------------------------------------------------------------------- */
+/* Spectral basis for the learned search's proposals (no counterpart in the */
+/* reference): out (cols x k, row-major) = the k leading eigenvectors of    */
+/* A^T A, each with its largest-magnitude component positive, by subspace   */
+/* iteration with a Rayleigh-Ritz step (cols <= 64, k <= 8; columns beyond  */
+/* cols are zero).  *iterations (may be NULL) gets the iterations used.     */
+ld_status ld_spectral_basis(const int64_t *a, int32_t rows, int32_t cols, int32_t k, double *out,
+                            int32_t *iterations);
+
+/* ---------------------------------------------------------------------- */
 /* Strategy verifier (no counterpart in the reference).  The value, on the   */
 /* matrix as read, of the labeling a strategy file records (the file of     */
 /* print_results, functions.h:371-412: one entry per input row, or per      */

@@ -119,6 +119,8 @@ SIGNATURES = [
     ("ld_symmetry_walk_at", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ld_solve_resumable", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
                                      C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, _I32P]),
+    ("ld_spectral_basis", C.c_int, [_I64P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_int32)]),
     ("ld_strategy_value", C.c_int, [C.c_char_p, C.c_size_t, C.c_int32, C.c_char, C.c_int32, _I32P, C.c_int32,
                                     _I64P]),
     ("ld_verify_main", C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
@@ -290,6 +292,17 @@ def symmetry_walk_at(d: int, prefix_digits: int, rank: int) -> int:
     w = C.c_uint64()
     _check(lib().ld_symmetry_walk_at(d, prefix_digits, rank, C.byref(w)))
     return int(w.value)
+
+
+def spectral_basis(a, k: int = 3) -> np.ndarray:
+    """The k leading eigenvectors of A^T A (cols x k, float64), each with
+    its largest-magnitude component positive (ld_spectral_basis)."""
+    a = _as_i64(a)
+    r, c = a.shape
+    out = np.zeros((c, k), dtype=np.float64)
+    _check(lib().ld_spectral_basis(a.ctypes.data_as(_I64P), r, c, k,
+                                   out.ctypes.data_as(C.POINTER(C.c_double)), None))
+    return out
 
 
 def strategy_value(text: str, d: int, stat: str = "n", marginal: bool = False, strategy=()) -> int:

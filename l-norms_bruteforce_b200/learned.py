@@ -56,8 +56,13 @@ def _pkg():
 
 def spectral_basis(a: np.ndarray, k: int = 3) -> np.ndarray:
     """Top-k right singular vectors (m x k) of a (rows x cols) matrix: the
-    eigenvectors of A^T A with the k largest eigenvalues (signs arbitrary;
-    a direction and its negation give the same labeling)."""
+    eigenvectors of A^T A with the k largest eigenvalues, from the library's
+    subspace iteration (ld_spectral_basis; each vector's largest component
+    positive).  A direction and its negation give the same labeling, so the
+    sign rule does not matter to the proposals.  Matrices wider than 64
+    columns use LAPACK through numpy."""
+    if a.shape[1] <= 64 and k <= 8:
+        return _pkg().spectral_basis(a, k)
     a = np.asarray(a, dtype=np.float64)
     _, u = np.linalg.eigh(a.T @ a)
     v = u[:, ::-1][:, :k]

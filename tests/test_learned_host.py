@@ -54,6 +54,40 @@ def test_row_features_layout(L):
         L.row_features(np.ones((45, 44)), v, dirs)
 
 
+def test_spectral_basis_matches_lapack(ld, L):
+    """The library's subspace iteration gives LAPACK's leading eigenvectors
+    of A^T A (up to sign) on the learned search's matrices, each with its
+    largest-magnitude component positive."""
+    for seed, n in ((1, 16), (2, 28), (3, 44), (4, 20)):
+        a = lowrank(seed, n)
+        v = ld.spectral_basis(a)
+        _, u = np.linalg.eigh(a.T.astype(np.float64) @ a.astype(np.float64))
+        ref = u[:, ::-1][:, :3]
+        np.testing.assert_allclose(np.abs(np.sum(v * ref, axis=0)), 1.0, atol=1e-9)
+        idx = np.argmax(np.abs(v), axis=0)
+        assert np.all(v[idx, np.arange(3)] > 0)
+        np.testing.assert_allclose(v.T @ v, np.eye(3), atol=1e-10)
+
+
+def test_spectral_basis_edge_cases(ld):
+    # rank 1 and 2: the leading vectors span the row space, the rest is an
+    # orthonormal completion
+    for rows in (1, 2):
+        a = np.random.default_rng(rows).integers(-5, 6, size=(rows, 12)).astype(np.int64)
+        v = ld.spectral_basis(a)
+        np.testing.assert_allclose(v.T @ v, np.eye(3), atol=1e-9)
+        g = a.T.astype(np.float64) @ a
+        top = np.linalg.eigvalsh(g)[::-1][:rows]
+        np.testing.assert_allclose(np.diag(v.T @ g @ v)[:rows], top, rtol=1e-9)
+    # a zero matrix and fewer columns than vectors
+    np.testing.assert_allclose(ld.spectral_basis(np.zeros((3, 5), dtype=np.int64)).T
+                               @ ld.spectral_basis(np.zeros((3, 5), dtype=np.int64)), np.eye(3), atol=1e-12)
+    v = ld.spectral_basis(np.array([[3, 4], [1, -2]], dtype=np.int64))
+    assert v.shape == (2, 3) and np.all(v[:, 2] == 0)
+    with pytest.raises(ld.LdError):
+        ld.spectral_basis(np.ones((3, 65), dtype=np.int64))
+
+
 def test_training_examples_are_aligned(L):
     mats = [lowrank(s, n) for s, n in ((3, 16), (4, 21), (5, 12))]
     signs = []
