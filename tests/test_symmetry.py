@@ -191,3 +191,15 @@ def test_library_walk_of_rank_long_prefixes(ld):
             w = ld.symmetry_walk_at(d, P, r)
             assert walk_ok(w, P, d)
             assert ld.symmetry_walks(d, P, 0, w) == r     # rank = passing walks below it
+
+
+def test_library_argument_checks(ld):
+    assert ld.symmetry_walk_ok(2, 10, 5) and ld.symmetry_walk_ok(1, 10, 7)     # d <= 2: every walk
+    assert not ld.symmetry_walk_ok(3, 2, 9)                                    # not a 2-digit number
+    with pytest.raises(ld.LdError):
+        ld.symmetry_walks(3, 4, 10, 5)                                         # lo > hi
+    with pytest.raises(ld.LdError):
+        ld.symmetry_walks(3, 4, 0, 3 ** 4 + 1)                                 # beyond d^P
+    with pytest.raises(ld.LdError):
+        ld.symmetry_walks(11, 2, 0, 1)                                         # d > 10
+    assert ld.symmetry_walk_at(2, 5, 7) == 7

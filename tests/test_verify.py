@@ -62,3 +62,20 @@ def test_verifier_finds_a_worse_strategy(ld):
     best = [int(x) for x in case["strategy"].split()]
     worse = [-x for x in best[:-1]] + best[-1:]
     assert ld.strategy_value(case["text"], d, stat, marg, worse) <= printed_value(case["stdout"])
+
+
+def test_verifier_hand_cases(ld):
+    # d = 1, no preprocessing: signs on rows
+    text = "1 2\n3 -4\n"
+    assert ld.strategy_value(text, 1, "n", False, [1, 1]) == abs(1 + 3) + abs(2 - 4)
+    assert ld.strategy_value(text, 1, "n", False, [1, -1]) == abs(1 - 3) + abs(2 + 4)
+    # LM: column 0 enters signed
+    assert ld.strategy_value(text, 1, "n", True, [1, -1]) == (1 - 3) + abs(2 + 4)
+    # d = 1 with more rows than columns is transposed: signs on columns
+    tall = "1 2\n3 4\n5 -6\n"
+    assert ld.strategy_value(tall, 1, "n", False, [1, -1]) == abs(1 - 2) + abs(3 - 4) + abs(5 + 6)
+    with pytest.raises(ld.LdError):
+        ld.strategy_value(tall, 1, "n", False, [1, -1, 1])                     # rows, not columns
+    # d = 3: labels group rows into messages
+    t3 = "1 0\n0 2\n3 3\n"
+    assert ld.strategy_value(t3, 3, "n", False, [0, 1, 1]) == 1 + 0 + 3 + 5
