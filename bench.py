@@ -47,10 +47,48 @@ def load_package():
     return mod
 
 
+def load_workloads():
+    """workloads.py on its own (it needs numpy only), so that the reference
+    arm never maps the solver library into its process."""
+    name = "lnorms_b200_workloads"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, PKG_DIR / "workloads.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def instance(cfg: int):
-    load_package()
-    import lnorms_b200.workloads as W
+    W = load_workloads()
     return {1: W.config1, 2: W.config2, 3: W.config3, 5: W.config5}[cfg]()
+
+
+def reduced_shape(inst) -> tuple[int, int]:
+    """Rows x columns left by the preprocessing: the generator's core for
+    configuration 2 (its planted copies unite and its zero rows vanish), the
+    input shape for the configurations without a flag (a d = 1 matrix with
+    more rows than columns is transposed)."""
+    if "core" in inst.meta:
+        return tuple(int(x) for x in inst.meta["core"])
+    r, c = inst.matrix.shape
+    return (c, r) if inst.d == 1 and r > c else (r, c)
+
+
+def workload_config(inst) -> dict:
+    """The `config` object of the bench line, identical in both arms: what
+    the workload is, not how an arm runs it."""
+    rows, cols = reduced_shape(inst)
+    base = 2 if inst.d <= 2 else inst.d
+    labelings = base ** (rows - 1)
+    flags = " ".join(inst.argv_tail()[1:]) or "none"
+    r0, c0 = inst.matrix.shape
+    return {"workload": (f"{inst.name}: {r0}x{c0} integer matrix, d={inst.d}"
+                         f"{' with marginals' if inst.marginal else ''}, flags {flags}; preprocessing leaves "
+                         f"{rows}x{cols}, {labelings} labelings"),
+            "rows": rows, "cols": cols, "d": inst.d, "marginal": bool(inst.marginal), "flags": flags,
+            "labelings_per_step": labelings,
+            "l2": "GPU arm: flushed between steps (512 MiB write outside the timed events); inputs of a few KB"}
 
 
 def ops_per_labeling(d: int, cols: int) -> int:
@@ -216,12 +254,24 @@ def reference_sample(inst, ld, target_labelings: int):
 
 
 def cpu_baseline(inst, ld, target_seconds: float = 15.0) -> dict:
+    """The reference's L_OpenMP on this host's cores: the full input file
+    when that takes at most about twice target_seconds (configuration 2:
+    about 4-11 s), else a bounded sample of the reduced matrix."""
     threads = os.cpu_count() or 1
     # calibrate on a small sample, then size the timed sample to ~target_seconds
     a, tail, n0, _ = reference_sample(inst, ld, 1 << 24)
     if REF_BIN.exists():
         t0, _ = run_reference_binary(a, tail, threads)
         rate = n0 / max(t0, 1e-3)
+        cfg = workload_config(inst)
+        n = cfg["labelings_per_step"]
+        if n / rate <= 2 * target_seconds:
+            t, out = run_reference_binary(inst.matrix, inst.argv_tail(), threads)
+            value_line, rows, cols = reference_output(out)
+            return {"value": n / t, "unit": "labelings/s", "cores": threads, "kind": "reference",
+                    "sample": f"L_OpenMP.c built from the reference sources, {threads} threads, the full "
+                              f"{inst.name} input file with flags {cfg['flags']} ({rows}x{cols} after its "
+                              f"preprocessing, {n} labelings, value {value_line}, {t:.2f} s)"}
         a, tail, n, what = reference_sample(inst, ld, int(rate * target_seconds))
         t, _ = run_reference_binary(a, tail, threads)
         return {"value": n / t, "unit": "labelings/s", "cores": threads, "kind": "reference",
@@ -243,45 +293,87 @@ def cpu_baseline(inst, ld, target_seconds: float = 15.0) -> dict:
             "sample": f"oracle restatement, {threads} threads, first {n} labelings of {inst.name}"}
 
 
+def reference_output(stdout: str) -> tuple[int, int, int]:
+    """(value, reduced rows, reduced columns) from the reference's stdout:
+    the `L.. is: v` line and the preprocessing messages (functions.h:76,
+    131-285): each removed zero line and each line united into another
+    takes one row or column off the matrix as read; a transposed matrix
+    swaps the two."""
+    value, rows, cols, dr, dc, transposed = None, None, None, 0, 0, False
+    gone = ("entries are zeros", "was added to", "was subtracted from")
+    for ln in stdout.splitlines():
+        s = ln.strip()
+        if s.startswith("rows:") and "cols:" in s:
+            rows = int(s.split(",")[0].split(":")[1])
+            cols = int(s.split("cols:")[1])
+        elif " is: " in s:
+            value = int(s.split(" is: ")[1])
+        elif s.startswith(("row ", "col ")) and any(m in s for m in gone):
+            if s.startswith("row "):
+                dr += 1
+            else:
+                dc += 1
+        elif s == "The entries of the first row and column are zeros.":
+            dr, dc = dr + 1, dc + 1   # the zero marginal row and column are dropped
+        elif s == "Matrix was transposed.":
+            transposed = True
+    if value is None or rows is None:
+        raise RuntimeError(f"unexpected reference output: {stdout[-300:]}")
+    rows, cols = rows - dr, cols - dc
+    return (value, cols, rows) if transposed else (value, rows, cols)
+
+
 def run_reference_arm(args) -> None:
+    """The reference's own OpenMP solver (L_OpenMP.c, compiled unmodified
+    from its sources into oracle/_ref/) on the full workload: each step runs
+    it once on the configuration's input file with the configuration's
+    flags (`L_OpenMP threads m.txt 1 y m` for configuration 2), so it reads,
+    preprocesses and enumerates every labeling itself.  This process loads
+    numpy and the workload generator only, never the solver library."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    ld = load_package()
     if args.config == 4 or args.method != "plain":
         print(json.dumps({"impl": "reference", "unavailable": "the reference solves one matrix per process "
                           "by plain enumeration; it has no batched or pruned form"}))
         return
-    inst = instance(args.config)
-    threads = os.cpu_count() or 1
     if not REF_BIN.exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/L_OpenMP was not built "
                           "(make -C oracle needs the reference sources)"}))
         return
-    # each step: a bounded sample of the workload sized to ~3 s on this host
-    a, tail, n0, _ = reference_sample(inst, ld, 1 << 24)
-    t0, _ = run_reference_binary(a, tail, threads)
-    rate = n0 / max(t0, 1e-3)
-    a, tail, n, what = reference_sample(inst, ld, int(rate * 3.0))
+    inst = instance(args.config)
+    cfg = workload_config(inst)
+    threads = os.cpu_count() or 1
+    tail = inst.argv_tail()
+    outs = []
     for _ in range(args.warmup):
-        run_reference_binary(a, tail, threads)
-    times = [run_reference_binary(a, tail, threads)[0] for _ in range(args.steps)]
+        run_reference_binary(inst.matrix, tail, threads)
+    times = []
+    for _ in range(args.steps):
+        dt, out = run_reference_binary(inst.matrix, tail, threads)
+        times.append(dt)
+        outs.append(reference_output(out))
+    value_line, rows, cols = outs[-1]
+    if (rows, cols) != (cfg["rows"], cfg["cols"]) or any(o != outs[0] for o in outs):
+        raise RuntimeError(f"reference reduced the workload to {rows}x{cols} (expected {cfg['rows']}x"
+                           f"{cfg['cols']}) or its steps disagree: {outs[:3]}")
     total = sum(times)
+    n = cfg["labelings_per_step"]
     value = n * args.steps / total
-    p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
-    info = p.info
-    sample = f"L_OpenMP.c built from the reference sources, {threads} threads, {what} ({n} labelings)"
+    sample = (f"L_OpenMP.c compiled unmodified from the reference sources, {threads} threads, the full "
+              f"{inst.name} input file with flags {cfg['flags']} per step ({n} labelings after its own "
+              f"preprocessing; printed value {value_line}); whole-process wall clock")
     line = {
         "impl": "reference", "metric": "exact L_d labelings/s (plain enumeration)", "value": value,
         "unit": "labelings/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator of the configuration)",
-        "config": {"workload": workload_name(inst, info), "rows": info["rows"], "cols": info["cols"],
-                   "d": info["d"], "marginal": bool(info["marginal"]), "labelings_per_step": n},
+        "config": cfg,
         "cpu_baseline": {"value": value, "unit": "labelings/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "labelings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "details": {"value": value_line, "reduced": [rows, cols]},
     }
     print(json.dumps(line))
 
@@ -390,10 +482,14 @@ def run_ours(args) -> None:
     ld = load_package()
     import lnorms_b200.distributed as D
     inst = instance(args.config)
+    cfg = workload_config(inst)
     prob = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
     info = prob.info
     red = prob.reduced
     d, marg = info["d"], bool(info["marginal"])
+    if (info["rows"], info["cols"], int(info["labelings"])) != (cfg["rows"], cfg["cols"], cfg["labelings_per_step"]):
+        raise RuntimeError(f"preprocessing left {info['rows']}x{info['cols']}, the workload says "
+                           f"{cfg['rows']}x{cfg['cols']}")
     opts = ld.options(device=local, shard_index=rank, shard_count=world)
     plan = ld.Plan(red, d, marg, opts)
     lo, hi = plan.range
@@ -404,14 +500,9 @@ def run_ours(args) -> None:
     def step():
         plan.launch()
 
-    def combine(val_idx):
-        # (value, index) -> global max value, smallest index attaining it
-        v = val_idx[0:1].clone()
-        dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        idx = torch.where(val_idx[0:1] == v, val_idx[1:2],
-                          torch.full_like(val_idx[1:2], torch.iinfo(torch.int64).max))
-        dist.all_reduce(idx, op=dist.ReduceOp.MIN)
-        return v, idx
+    # the cross-rank (value, Gray index) combine: distributed.combine_tensor,
+    # on the plan's device result slot, queued on the solver's stream
+    combine = D.combine_tensor
 
     # the plan's result slot, viewed as a tensor for the cross-rank combine
     res_view = None
@@ -488,15 +579,13 @@ def run_ours(args) -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator of the configuration)",
-            "config": {"workload": workload_name(inst, info), "rows": info["rows"], "cols": info["cols"],
-                       "d": d, "marginal": marg, "labelings_per_step": total_labelings,
-                       "evaluated_per_step": evaluated if world == 1 else None,
-                       "label_symmetry": (f"{evaluated / (hi - lo):.4f} of the labelings evaluated: walks that "
-                                          f"hold no smallest index of a class under permutations of labels "
-                                          f"1..{d - 1} are skipped") if d >= 3 and evaluated < hi - lo else None,
-                       "parallelism": f"gray-index shards x{world}" if world > 1 else "single GPU",
-                       "l2": "flushed between steps (512 MiB write outside the timed events)",
-                       "kernel": desc, "value": sol.value, "gray_index": sol.gray_index},
+            "config": cfg,
+            "details": {"evaluated_per_step": evaluated if world == 1 else None,
+                        "label_symmetry": (f"{evaluated / (hi - lo):.4f} of the labelings evaluated: walks that "
+                                           f"hold no smallest index of a class under permutations of labels "
+                                           f"1..{d - 1} are skipped") if d >= 3 and evaluated < hi - lo else None,
+                        "parallelism": f"gray-index shards x{world}" if world > 1 else "single GPU",
+                        "kernel": desc, "value": sol.value, "gray_index": sol.gray_index},
             "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12,
                          "unit": "Tops/s", "frac": achieved / peak_ops,
                          "traffic": TRAFFIC_BYTES.get(args.config) if world == 1 else None,
@@ -515,12 +604,63 @@ def run_ours(args) -> None:
         }
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(inst, ld)
+        if world == 1 and args.config5_count > 0:
+            line["config5"] = config5_leg(ld, local, args.config5_count, steps=3, warmup=2)
         assert sol0.value == sol.value and sol0.gray_index == sol.gray_index
         print(json.dumps(line))
     plan.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def config5_leg(ld, local: int, count: int, steps: int, warmup: int) -> dict:
+    """The metric's other half, on configuration 5 (44x44 low rank, L_1,
+    2^43 labelings): one plain enumeration against the exact learned-pruned
+    search, batched over `count` matrices of the same distribution (seeds
+    5 .. 5 + count - 1; seed 5 is configuration 5 itself), with network
+    proposals and, as the method without the network, uniform random ones.
+    Times are wall clock per matrix from host matrix to host answer, taken
+    after the configuration-2 events; the answer for configuration 5 must
+    equal the plain enumeration's (value and Gray index)."""
+    import lnorms_b200.learned as L
+
+    W = load_workloads()
+    inst = W.config5()
+    red = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal).reduced
+    plan = ld.Plan(red, 1, False, ld.options(device=local))
+    t0 = time.perf_counter()
+    ref = plan.solve()
+    plain_s = time.perf_counter() - t0
+    desc = plan.describe()
+    plan.close()
+    mats = [ld.Problem.from_matrix(W.config5(seed=5 + i).matrix, 1).reduced for i in range(count)]
+    total = 2 ** (red.shape[0] - 1)
+    out = {"workload": f"{inst.name}: {red.shape[0]}x{red.shape[1]}, {total} labelings per matrix",
+           "plain": {"s_per_matrix": plain_s, "kernel_ms": ref.kernel_ms, "labelings_per_s": total / plain_s,
+                     "kernel": desc, "value": ref.value, "gray_index": ref.gray_index},
+           "batch": count, "proposals_per_matrix": 8}
+    for mode, key in (("network", "learned_pruned"), ("random", "random_pruned")):
+        proposer = L.Proposer(mode, directions=8, samples=1, device=local)
+        for _ in range(warmup):
+            res = L.solve_learned_batch(mats, proposer)
+        walls = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            res = L.solve_learned_batch(mats, proposer)
+            walls.append(time.perf_counter() - t0)
+        proposer.close()
+        first = res[0][0]
+        if (first.value, first.gray_index) != (ref.value, ref.gray_index):
+            raise AssertionError(f"{key}: {(first.value, first.gray_index)} != plain "
+                                 f"{(ref.value, ref.gray_index)}")
+        ms = 1e3 * statistics.mean(walls) / count
+        out[key] = {"ms_per_matrix": ms, "speedup_vs_plain": plain_s * 1e3 / ms,
+                    "labelings_per_s": total / (ms * 1e-3),
+                    "walks_kept_mean": statistics.mean(r[1]["prune_walks_kept"] for r in res),
+                    "incumbent_optimal": sum(int(r[1]["incumbent"] == r[0].value) for r in res)}
+    out["target"] = "learned-pruned >= 5x faster than the plain GPU enumeration"
+    return out
 
 
 def run_batch(args) -> None:
@@ -754,6 +894,9 @@ def main() -> None:
                     help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")
     ap.add_argument("--ref-launch", default="",
                     help="reference-gpu: blocks x threads to use (e.g. 9472x256) instead of the sweep")
+    ap.add_argument("--config5-count", type=int, default=32,
+                    help="plain runs: also time configuration 5, plain against the batched learned- and "
+                         "random-pruned exact search over this many matrices (0 = skip)")
     ap.add_argument("--with-plain", action="store_true",
                     help="also time one plain enumeration of the workload (pruned / learned)")
     args = ap.parse_args()

@@ -163,12 +163,16 @@ ld_status ld_solve_reduced(const int64_t *mtx_as_vec, int32_t rows, int32_t cols
  * synchronize the device, and fail once another framework in the process
  * holds nearly all of its memory): all device working memory is one 64 KiB
  * file-scope __device__ array, reserved on every GPU that loads the library.
- * Host matrix in, host result out; `stream` may be NULL.  Limits: d <= 3,
- * <= 63 rows, <= 64 columns (<= 128 when every partial column sum fits in 8
- * bits), column sums within 32 bits; larger inputs get LD_ERR_LIMIT.  The
- * first call on a device looks up the array's address (make it before any
- * stream capture on that device).  Calls share the array and are serialised
- * by a host lock; GPU work of two calls must not overlap.  kernel_ms is 0. */
+ * Host matrix in, host result out.  `stream` NULL means the legacy default
+ * stream, which synchronises with every blocking stream of the device; pass
+ * a cudaStreamNonBlocking stream to keep other work running.  Each call
+ * waits for its stream before returning.  Limits: d <= 3, <= 63 rows,
+ * <= 64 columns (<= 128 when every partial column sum fits in 8 bits),
+ * column sums within 32 bits; larger inputs get LD_ERR_LIMIT.  At d = 3 it
+ * skips the same label-permuted walks as ld_solve_reduced.  The first call
+ * on a device looks up the array's address (make it before any stream
+ * capture on that device).  Calls share the array and are serialised by a
+ * host lock; GPU work of two calls must not overlap.  kernel_ms is 0. */
 ld_status ld_solve_reduced_noalloc(const int64_t *mtx_as_vec, int32_t rows, int32_t cols,
                                    int32_t d, int32_t marginal, int32_t device, void *stream,
                                    ld_result *res, int32_t *strategy);

@@ -28,14 +28,18 @@ using namespace ldsolve;
 #include <tuple>
 
 #include "../kernels/batch_kernel.cuh"
+#include "device_guard.h"
 
 namespace {
+
+// threads per CTA the autotuner tries
+constexpr int kTpbChoices[3] = {64, 128, 256};
 
 struct BatchClass {
   int D = 0, WB = 0, WA = 0;
   const void* kfn = nullptr;
   size_t smem = 0;
-  int bps = 1;
+  int bps = 1;                    // resident CTAs per SM at tpb threads (plain instance)
   std::vector<int> probs;         // problem indices, largest first
   int wpt = 1;                    // walks per thread per chunk
   double grid_frac = 1.0;         // persistent CTAs per SM, as a fraction of the occupancy limit
@@ -43,19 +47,25 @@ struct BatchClass {
   size_t smem_split = 0;
   int bps_split = 0;
   bool split = false;             // the autotuner chose the column-split instance
+  int tpb = ld::kBatchThreads;    // threads per CTA (chunks hold tpb * wpt walks)
+  int occ[2][3] = {{0, 0, 0}, {0, 0, 0}};  // resident CTAs per SM: [split][kTpbChoices index]
   float tuned[2] = {0.f, 0.f};    // autotuner: best ms per 1e9 labelings, plain / split instance
   const void* fn() const { return split ? kfn_split : kfn; }
   size_t shm() const { return split ? smem_split : smem; }
-  int blocks_per_sm() const { return split ? bps_split : bps; }
+  int blocks_per_sm() const {
+    for (int t = 0; t < 3; ++t)
+      if (kTpbChoices[t] == tpb) return occ[split ? 1 : 0][t];
+    return 0;
+  }
   int chunk_first = 0, nchunks = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
 };
 
 // autotuner cache: (D, WB, WA, log2 of the mean walks per problem, batch_split option)
-//   -> (wpt, grid fraction, split)
+//   -> (wpt, grid fraction, split, threads per CTA)
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool>> g_tune;
+std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool, int>> g_tune;
 
 }  // namespace
 
@@ -104,7 +114,7 @@ static void batch_free(ld_batch* b) {
 // chunks of one class for a given walks-per-thread; returns the number of chunks
 static int batch_chunks(const ld_batch* b, const BatchClass& c, int wpt,
                         const std::vector<unsigned long long>& walks, std::vector<ld::BatchChunk>* out) {
-  const unsigned long long span = (unsigned long long)ld::kBatchThreads * (unsigned long long)wpt;
+  const unsigned long long span = (unsigned long long)c.tpb * (unsigned long long)wpt;
   int n = 0;
   for (int p : c.probs) {
     for (unsigned long long w = 0; w < walks[p]; w += span) {
@@ -124,6 +134,7 @@ static int batch_chunks(const ld_batch* b, const BatchClass& c, int wpt,
 extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, const int32_t* rows,
                                      const int32_t* cols, const int32_t* ds, const int32_t* margs,
                                      const ld_options* opt, int32_t autotune, ld_batch** out) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!out || count < 1 || !mats || !rows || !cols || !ds) return ld_fail(LD_ERR_ARG, "bad batch arguments");
   ld_options o;
   if (opt) o = *opt; else ld_options_init(&o);
@@ -270,19 +281,25 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   for (auto& c : b->classes) {
     std::stable_sort(c.probs.begin(), c.probs.end(),
                      [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
-    if (ld_raise_smem_limit(c.kfn, c.smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps, c.kfn, ld::kBatchThreads, c.smem) != cudaSuccess ||
-        c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+    bool ok = ld_raise_smem_limit(c.kfn, c.smem) == cudaSuccess;
+    for (int t = 0; t < 3 && ok; ++t)
+      ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ[0][t], c.kfn, kTpbChoices[t], c.smem) == cudaSuccess;
+    c.bps = c.occ[0][1];
+    if (!ok || c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
       batch_free(b);
       return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d WA=%d does not fit an SM", c.D, c.WB, c.WA);
     }
-    if (c.kfn_split && (ld_raise_smem_limit(c.kfn_split, c.smem_split) != cudaSuccess ||
-                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.bps_split, c.kfn_split, ld::kBatchThreads,
-                                                                      c.smem_split) != cudaSuccess ||
-                        c.bps_split < 1)) {
-      cudaGetLastError();
-      c.kfn_split = nullptr;
+    if (c.kfn_split) {
+      bool sok = ld_raise_smem_limit(c.kfn_split, c.smem_split) == cudaSuccess;
+      for (int t = 0; t < 3 && sok; ++t)
+        sok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ[1][t], c.kfn_split, kTpbChoices[t],
+                                                            c.smem_split) == cudaSuccess;
+      c.bps_split = c.occ[1][1];
+      if (!sok || c.bps_split < 1) {
+        cudaGetLastError();
+        c.kfn_split = nullptr;
+      }
     }
   }
   // device memory: images, problem table, chunks (sized for the largest wpt
@@ -292,8 +309,12 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   std::vector<size_t> img_off(count, 0);
   for (int p = 0; p < count; ++p)
     if (b->cls[p] >= 0) { img_off[p] = bytes; bytes += align256(images[p].size()); }
-  int max_chunks = 0;
-  for (auto& c : b->classes) max_chunks += batch_chunks(b, c, 1, walks, nullptr);
+  int max_chunks = 0;   // the most chunks any candidate makes: 64 threads, 1 walk each
+  for (auto& c : b->classes) {
+    BatchClass tc = c;
+    tc.tpb = kTpbChoices[0];
+    max_chunks += batch_chunks(b, tc, 1, walks, nullptr);
+  }
   b->off_prob = bytes;   bytes += align256(sizeof(ld::BatchProblem) * count);
   b->off_chunks = bytes; bytes += align256(sizeof(ld::BatchChunk) * std::max(1, max_chunks));
   b->off_heads = bytes;  bytes += align256(sizeof(unsigned int) * std::max<size_t>(1, b->classes.size()));
@@ -356,9 +377,64 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     return std::min(g, std::max(1, c.nchunks));
   };
 
-  // autotuner: walks per thread per chunk and the persistent grid size, timed
-  // on one wave of each class's chunks from its median matrix on; cached per
-  // class shape and matrix size.
+  // autotuner: per class, the instance (plain or column-split), threads per
+  // CTA (64, 128, 256), walks per thread per chunk (1, 2, 4, 8; the chunk
+  // holds threads x walks walks) and the persistent grid (half or all of the
+  // occupancy limit), timed on one wave of the class's chunks from its
+  // median matrix on and normalised per labeling.  Every candidate is timed
+  // once; the four fastest are timed three more times and the best median
+  // wins (the first launch of an instance also loads its module).  Cached
+  // per class shape and matrix size.
+  struct Cand { int variant, tpb, wpt; double frac; float per; };
+  auto time_cand = [&](BatchClass& c, Cand& cd, int reps, float* per_out) -> ld_status {
+    BatchClass tc = c;
+    tc.split = cd.variant == 1;
+    tc.tpb = cd.tpb;
+    tc.grid_frac = cd.frac;
+    const int bps = tc.blocks_per_sm();
+    *per_out = 1e30f;
+    if (bps < 1) return LD_OK;            // this shape does not fit an SM
+    std::vector<ld::BatchChunk> all;
+    batch_chunks(b, tc, cd.wpt, walks, &all);
+    // one wave of chunks (a chunk per resident CTA), starting at the
+    // class's median matrix: the class's steady state at a fraction of the
+    // cost of its largest matrices
+    const int wave = di.sms * bps;
+    size_t first = 0;
+    const int median = c.probs[c.probs.size() / 2];
+    while (first < all.size() && all[first].problem != median) ++first;
+    if (first + (size_t)wave > all.size()) first = all.size() > (size_t)wave ? all.size() - wave : 0;
+    const int sample = std::min<int>((int)(all.size() - first), wave);
+    if (sample < 1) return LD_OK;
+    LD_CUDA(cudaMemcpy(b->dmem + b->off_chunks, all.data() + first, sizeof(ld::BatchChunk) * sample,
+                       cudaMemcpyHostToDevice));
+    tc.chunk_first = 0;
+    tc.nchunks = sample;
+    ld::BatchArgs args = class_args(c);
+    args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks);
+    args.nchunks = sample;
+    args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres);
+    std::vector<float> ms(reps, 0.f);
+    for (int rep = 0; rep < reps; ++rep) {
+      LD_CUDA(cudaMemsetAsync(args.head, 0, sizeof(unsigned int), b->stream));
+      LD_CUDA(cudaEventRecord(b->ev0, b->stream));
+      void* params[] = {&args};
+      LD_CUDA(cudaLaunchKernel(tc.fn(), dim3(class_grid(tc)), dim3(tc.tpb), params, tc.shm(), b->stream));
+      LD_CUDA(cudaEventRecord(b->ev1, b->stream));
+      LD_CUDA(cudaEventSynchronize(b->ev1));
+      LD_CUDA(cudaEventElapsedTime(&ms[rep], b->ev0, b->ev1));
+    }
+    std::sort(ms.begin(), ms.end());
+    // normalise by the labelings the sample covered
+    double lab = 0;
+    for (int i = 0; i < sample; ++i) {
+      const ld::BatchChunk& q = all[first + i];
+      lab += (double)(q.walk_end - q.walk_begin) * (double)b->hprob[q.problem].walk_len *
+             (double)b->hprob[q.problem].B;
+    }
+    *per_out = (float)(ms[reps / 2] / std::max(1.0, lab));
+    return LD_OK;
+  };
   for (auto& c : b->classes) {
     double mean = 0;
     for (int p : c.probs) mean += (double)walks[p];
@@ -368,65 +444,38 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune.find(key);
       if (it != g_tune.end()) {
-        std::tie(c.wpt, c.grid_frac, c.split) = it->second;
+        std::tie(c.wpt, c.grid_frac, c.split, c.tpb) = it->second;
         if (!c.kfn_split) c.split = false;
         if (o.batch_split > 0 && c.kfn_split) c.split = true;
+        if (c.blocks_per_sm() < 1) { c.tpb = ld::kBatchThreads; }
         continue;
       }
     }
     if (o.batch_split > 0 && c.kfn_split) c.split = true;
     if (!autotune) continue;
-    float best_ms = 1e30f;
-    int best_wpt = 1;
-    double best_frac = 1.0;
-    bool best_split = false;
+    std::vector<Cand> cands;
     for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
-    for (int wpt : {1, 2, 4, 8}) {
-      for (double frac : {0.5, 1.0}) {   // persistent CTAs: half or all of the occupancy limit
-        std::vector<ld::BatchChunk> all;
-        batch_chunks(b, c, wpt, walks, &all);
-        // one wave of chunks (a chunk per resident CTA), starting at the
-        // class's median matrix: the class's steady state at a fraction of
-        // the cost of its largest matrices
-        const int wave = di.sms * (variant ? c.bps_split : c.bps);
-        size_t first = 0;
-        const int median = c.probs[c.probs.size() / 2];
-        while (first < all.size() && all[first].problem != median) ++first;
-        if (first + (size_t)wave > all.size()) first = all.size() > (size_t)wave ? all.size() - wave : 0;
-        std::vector<ld::BatchChunk> chunks(all.begin() + first, all.end());
-        const int sample = std::min<int>((int)chunks.size(), wave);
-        if (sample < 1) continue;
-        cudaMemcpy(b->dmem + b->off_chunks, chunks.data(), sizeof(ld::BatchChunk) * sample, cudaMemcpyHostToDevice);
-        BatchClass tc = c;
-        tc.chunk_first = 0; tc.nchunks = sample; tc.grid_frac = frac; tc.split = variant == 1;
-        ld::BatchArgs args = class_args(c);
-        args.chunks = (const ld::BatchChunk*)(b->dmem + b->off_chunks);
-        args.nchunks = sample;
-        args.chunk_results = (ld::Slot*)(b->dmem + b->off_cres);
-        float ms = 0;
-        for (int rep = 0; rep < 1; ++rep) {
-          cudaMemsetAsync(args.head, 0, sizeof(unsigned int), b->stream);
-          cudaEventRecord(b->ev0, b->stream);
-          void* params[] = {&args};
-          cudaLaunchKernel(tc.fn(), dim3(class_grid(tc)), dim3(ld::kBatchThreads), params, tc.shm(), b->stream);
-          cudaEventRecord(b->ev1, b->stream);
-          cudaEventSynchronize(b->ev1);
-          cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-        }
-        // normalize by the labelings the sample covered
-        double lab = 0;
-        for (int i = 0; i < sample; ++i)
-          lab += (double)(chunks[i].walk_end - chunks[i].walk_begin) * (double)b->hprob[chunks[i].problem].walk_len *
-                 (double)b->hprob[chunks[i].problem].B;
-        const float per = (float)(ms / std::max(1.0, lab));
-        if (per < best_ms) { best_ms = per; best_wpt = wpt; best_frac = frac; best_split = variant == 1; }
-        if (c.tuned[variant] == 0.f || per * 1e9f < c.tuned[variant]) c.tuned[variant] = per * 1e9f;
-      }
+      for (int tpb : kTpbChoices)
+        for (int wpt : {1, 2, 4, 8})
+          for (double frac : {0.5, 1.0}) cands.push_back(Cand{variant, tpb, wpt, frac, 1e30f});
+    for (auto& cd : cands) {
+      st = time_cand(c, cd, 1, &cd.per);
+      if (st != LD_OK) { batch_free(b); return st; }
     }
-    if (cudaGetLastError() != cudaSuccess) { batch_free(b); return ld_fail(LD_ERR_CUDA, "autotune launch failed"); }
-    c.wpt = best_wpt; c.grid_frac = best_frac; c.split = best_split;
+    std::sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.per < y.per; });
+    const size_t top = std::min<size_t>(4, cands.size());
+    for (size_t i = 0; i < top; ++i) {
+      st = time_cand(c, cands[i], 3, &cands[i].per);
+      if (st != LD_OK) { batch_free(b); return st; }
+    }
+    std::sort(cands.begin(), cands.begin() + top, [](const Cand& x, const Cand& y) { return x.per < y.per; });
+    for (const auto& cd : cands)
+      if (c.tuned[cd.variant] == 0.f || cd.per * 1e9f < c.tuned[cd.variant]) c.tuned[cd.variant] = cd.per * 1e9f;
+    if (!cands.empty() && cands[0].per < 1e29f) {
+      c.wpt = cands[0].wpt; c.grid_frac = cands[0].frac; c.split = cands[0].variant == 1; c.tpb = cands[0].tpb;
+    }
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[key] = std::make_tuple(best_wpt, best_frac, best_split);
+    g_tune[key] = std::make_tuple(c.wpt, c.grid_frac, c.split, c.tpb);
   }
   st = build_queue();
   if (st != LD_OK) { batch_free(b); return st; }
@@ -442,7 +491,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     ld::BatchArgs args = class_args(c);
     void* params[] = {&args};
     if (e == cudaSuccess && c.nchunks > 0)
-      e = cudaLaunchKernel(c.fn(), dim3(class_grid(c)), dim3(ld::kBatchThreads), params, c.shm(), c.stream);
+      e = cudaLaunchKernel(c.fn(), dim3(class_grid(c)), dim3(c.tpb), params, c.shm(), c.stream);
     if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
   }
   ld_status pst = LD_OK;
@@ -476,8 +525,8 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
            b->hchunks.size(), (int)std::count_if(b->plans.begin(), b->plans.end(), [](ld_plan* q) { return q != nullptr; }));
   b->desc = buf;
   for (auto& c : b->classes) {
-    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, grid=%d%s", c.D, c.WB, c.WA,
-             c.probs.size(), c.nchunks, c.wpt, class_grid(c), c.split ? ", column split" : "");
+    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, tpb=%d, grid=%d%s", c.D,
+             c.WB, c.WA, c.probs.size(), c.nchunks, c.wpt, c.tpb, class_grid(c), c.split ? ", column split" : "");
     b->desc += buf;
     if (c.tuned[0] > 0.f && c.tuned[1] > 0.f) {
       snprintf(buf, sizeof buf, " (tuned ms per 1e9 labelings: %.3f, split %.3f)", c.tuned[0], c.tuned[1]);
@@ -489,6 +538,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
 }
 
 extern "C" ld_status ld_batch_launch(ld_batch* b) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!b || !b->exec) return ld_fail(LD_ERR_ARG, "null batch");
   LD_CUDA(cudaSetDevice(b->device));
   // timing events outside the graph (events recorded during capture cannot be timed)
@@ -500,6 +550,7 @@ extern "C" ld_status ld_batch_launch(ld_batch* b) {
 }
 
 extern "C" ld_status ld_batch_results(ld_batch* b, int64_t* values, uint64_t* gray_indices, float* ms) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!b || !values) return ld_fail(LD_ERR_ARG, "null argument");
   if (!b->launched) return ld_fail(LD_ERR_ARG, "batch has not been launched");
   LD_CUDA(cudaSetDevice(b->device));
@@ -528,4 +579,7 @@ extern "C" ld_status ld_batch_evaluated(const ld_batch* b, uint64_t* evaluated) 
   return LD_OK;
 }
 
-extern "C" void ld_batch_destroy(ld_batch* b) { batch_free(b); }
+extern "C" void ld_batch_destroy(ld_batch* b) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
+  batch_free(b);
+}

@@ -12,6 +12,7 @@
 
 #include "../host/ld_internal.h"
 #include "../kernels/mlp_tc.cuh"
+#include "device_guard.h"
 
 namespace {
 
@@ -248,6 +249,7 @@ ld_status finish(ld_mlp* n) {
 }  // namespace
 
 extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int32_t device, ld_mlp** out) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!out || batch < 128 || batch % 128) return ld_fail(LD_ERR_ARG, "batch must be a positive multiple of 128");
   if (cudaSetDevice(device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "no device %d", device);
   ld_mlp* n = new ld_mlp();
@@ -340,6 +342,7 @@ extern "C" ld_status ld_mlp_create(int32_t batch, uint64_t seed, float skip, int
 }
 
 extern "C" void ld_mlp_destroy(ld_mlp* n) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!n) return;
   cudaSetDevice(n->device);
   if (n->s) cudaStreamSynchronize(n->s);
@@ -354,6 +357,7 @@ extern "C" void ld_mlp_destroy(ld_mlp* n) {
 extern "C" int64_t ld_mlp_param_count(void) { return (int64_t)host_param_count(); }
 
 extern "C" ld_status ld_mlp_get_params(ld_mlp* n, float* params) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!n || !params) return ld_fail(LD_ERR_ARG, "null argument");
   MLP_CUDA(cudaSetDevice(n->device));
   MLP_CUDA(cudaStreamSynchronize(n->s));
@@ -369,6 +373,7 @@ extern "C" ld_status ld_mlp_get_params(ld_mlp* n, float* params) {
 }
 
 extern "C" ld_status ld_mlp_set_params(ld_mlp* n, const float* params) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!n || !params) return ld_fail(LD_ERR_ARG, "null argument");
   MLP_CUDA(cudaSetDevice(n->device));
   const float* src = params;
@@ -385,6 +390,7 @@ extern "C" ld_status ld_mlp_set_params(ld_mlp* n, const float* params) {
 }
 
 extern "C" ld_status ld_mlp_forward(ld_mlp* n, const float* x, int32_t rows, float* logits) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!n || !x || !logits || rows < 1) return ld_fail(LD_ERR_ARG, "bad arguments");
   MLP_CUDA(cudaSetDevice(n->device));
   for (int r0 = 0; r0 < rows; r0 += n->batch) {
@@ -403,6 +409,7 @@ extern "C" ld_status ld_mlp_forward(ld_mlp* n, const float* x, int32_t rows, flo
 // gradients of the mean masked BCE loss (flat host layout), no update
 extern "C" ld_status ld_mlp_gradients(ld_mlp* n, const float* x, const float* t, const float* mask, int32_t rows,
                                       float* grads, float* loss) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!n || !x || !t || !mask || rows < 1 || rows > n->batch) return ld_fail(LD_ERR_ARG, "bad arguments");
   MLP_CUDA(cudaSetDevice(n->device));
   n->hHp[ld::mlp::kHpInvCount] = stage_batch(n, x, t, mask, rows);
@@ -430,6 +437,7 @@ extern "C" ld_status ld_mlp_gradients(ld_mlp* n, const float* x, const float* t,
 // One Adam step: a single launch of the captured training graph.
 extern "C" ld_status ld_mlp_train_step(ld_mlp* n, const float* x, const float* t, const float* mask, int32_t rows,
                                        float lr, float* loss) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!n || !x || !t || !mask || rows < 1 || rows > n->batch) return ld_fail(LD_ERR_ARG, "bad arguments");
   MLP_CUDA(cudaSetDevice(n->device));
   n->step += 1;
@@ -448,6 +456,7 @@ extern "C" ld_status ld_mlp_train_step(ld_mlp* n, const float* x, const float* t
 // C[M x N] = A[M x K] * B[N x K]^T, M % 128 == 0, N % 64 == 0, K % 64 == 0.
 extern "C" ld_status ld_tc_gemm(const uint16_t* A, const uint16_t* B, int32_t M, int32_t N, int32_t K, float* C,
                                 int32_t device) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!A || !B || !C || M < 128 || M % 128 || N < 64 || N % 64 || K < 64 || K % 64)
     return ld_fail(LD_ERR_ARG, "shape must be M%%128, N%%64, K%%64");
   MLP_CUDA(cudaSetDevice(device));

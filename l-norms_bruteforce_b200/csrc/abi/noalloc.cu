@@ -23,6 +23,12 @@
 // cudaGetSymbolAddress, once; make the first call on a device before any
 // stream capture on it.
 //
+// Stream: the work goes to the caller's stream; NULL means the legacy
+// default stream, which waits for (and holds up) every blocking stream of
+// the device, so a caller that must not stall other work passes a stream
+// created with cudaStreamNonBlocking.  Every call waits for its stream to
+// finish before it returns the result.
+//
 // Sharing: every call uses the same array and it keeps the previous call's
 // contents.  Each call rewrites the image and the counter / running-maximum
 // words that must start at 0 / INT64_MIN.  Calls from host threads of this
@@ -32,9 +38,12 @@
 // example from code that bypasses this function's lock) would race on it.
 //
 // Limit: the table kernel only (d <= 3; up to 64 columns in 32-bit lanes,
-// 128 in 8-bit lanes; at most 63 rows), so that the image (at most 16.5 KiB)
-// and one 16-byte slot per block fit in the 64 KiB array.  Anything larger
-// is rejected with LD_ERR_LIMIT before any device work.
+// 128 in 8-bit lanes; at most 63 rows), so that the image (at most 16.5 KiB),
+// the label-symmetry counts of d = 3 (at most 2.5 KiB) and one 16-byte slot per
+// block fit in the 64 KiB array.  Anything larger is rejected with
+// LD_ERR_LIMIT before any device work.  The work is ld_solve_reduced's: at
+// d = 3 the walks that cannot hold the smallest index of a class of
+// label-permuted labelings are skipped there too.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,6 +56,7 @@
 #include "../kernels/common.cuh"
 #include "../kernels/registry.h"
 #include "../kernels/table_kernel.cuh"
+#include "device_guard.h"
 
 namespace {
 
@@ -56,10 +66,18 @@ constexpr size_t kNoallocScratchBytes = 64 * 1024;
 // uses the address returned by cudaGetSymbolAddress.
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
-// image layout (same offsets as the allocating path's upload image)
+// image layout: the allocating path's upload image without its table-bias
+// block, so the rows start at 768.  No bias is needed: for LM the whole shift
+// K = sum |A_i0| goes into the initial high sums (h0[0] += K) and is
+// subtracted from the value; the table then holds the low rows' signed part
+// alone, which stays within 8 bits whenever 8-bit lanes are chosen
+// (2K <= 127).  The d = 3 label-symmetry counts follow the rows, 256-byte
+// aligned.
 constexpr size_t kCounter = 0, kGvalue = 8, kResult = 16;
 constexpr size_t kTot = 256, kH0 = 512, kA = 768;
-constexpr size_t kMaxImage = kA + 63 * 64 * 4;   // 63 rows x 64 words
+constexpr size_t kMaxRows = kA + 63 * 64 * 4;     // 63 rows x 64 words
+constexpr size_t kMaxSym = 4096;                  // d = 3: 8 (P + 1) counts of 8 bytes, P <= 39
+constexpr size_t kMaxImage = ((kMaxRows + 255) & ~(size_t)255) + kMaxSym;
 
 std::mutex g_mu[64];
 void* g_scratch[64];          // device address of the array, per device
@@ -93,6 +111,7 @@ unsigned long long ipow(unsigned long long b, int e) {
 extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32_t C, int32_t d,
                                               int32_t marginal, int32_t device, void* stream,
                                               ld_result* res, int32_t* strategy) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!a || !res || R < 1 || C < 1) return ld_fail(LD_ERR_ARG, "bad arguments");
   if (d < 1 || d > 3) return ld_fail(LD_ERR_LIMIT, "no-allocation solve takes d = 1, 2 or 3 (got %d)", d);
   if (marginal && d != 1) return ld_fail(LD_ERR_ARG, "marginals need d == 1");
@@ -122,8 +141,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   if (maxabs <= 127 && (C + 3) / 4 <= 32) { PK = 4; W = (((C + 3) / 4) + 3) & ~3; }
   else {
     PK = 1; W = (C + 3) & ~3;
-    const int wmax = d == 1 ? 64 : d == 2 ? 48 : 32;
-    if (W > wmax) return ld_fail(LD_ERR_LIMIT, "no-allocation solve takes at most %d columns for d=%d (got %d)", wmax, d, C);
+    if (W > 64) return ld_fail(LD_ERR_LIMIT, "no-allocation solve takes at most 64 columns (got %d)", C);
   }
   const void* kfn = ld::table_kernel_ptr(d, W, PK);
   if (!kfn) return ld_fail(LD_ERR_LIMIT, "no table kernel for d=%d and %d columns", d, C);
@@ -158,16 +176,34 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   if (e != cudaSuccess || bps < 1) return ld_fail(LD_ERR_CUDA, "occupancy query failed");
   const unsigned long long full = (unsigned long long)g_sms[device] * bps * ld::kTableThreads;
   const int nh = F - k;
+  // d = 3: only the walks that can hold a class minimum run (label
+  // symmetry), handed out by rank; the walk length follows the allocating
+  // path's rule (walks that run >= 16 per thread of a full grid for d <= 2,
+  // >= 4 for d = 3)
+  const bool sym = d >= 3;
+  auto walks_run = [&](int f) -> unsigned long long {
+    uint64_t c = ipow(base, nh - f);
+    if (sym && nh - f > 0 && ld_symmetry_walks(d, nh - f, 0, c, &c) != LD_OK) c = ipow(base, nh - f);
+    return (unsigned long long)c;
+  };
+  const unsigned long long per_thread = d >= 3 ? 4ull : 16ull;
   int fw = 0;
-  while (fw < nh && ipow(base, nh - fw - 1) >= 32ull * full) ++fw;
+  while (fw < nh && walks_run(fw + 1) >= per_thread * full) ++fw;
   const unsigned long long walk_len = ipow(base, fw), walks = ipow(base, nh - fw);
-  const size_t image = kA + (size_t)R * W * 4;
+  const int P = sym ? nh - fw : 0;
+  const unsigned long long run = walks_run(fw);
+  const size_t rows_end = kA + (size_t)R * W * 4;
+  const size_t sym_off = up256(rows_end);
+  const size_t sym_bytes = P > 0 ? ld_sym_table_len(d, P) * sizeof(uint64_t) : 0;
+  const size_t image = P > 0 ? sym_off + sym_bytes : rows_end;
+  if (rows_end > kMaxRows || sym_bytes > kMaxSym || image > kMaxImage)
+    return ld_fail(LD_ERR_LIMIT, "matrix image exceeds the scratch array");
   const size_t off_slots = up256(image);
   const unsigned long long max_blocks = (kNoallocScratchBytes - off_slots) / sizeof(ld::Slot);
   unsigned long long blocks = std::min<unsigned long long>((unsigned long long)g_sms[device] * bps,
-                                                           std::max(1ull, (walks + ld::kTableThreads - 1) / ld::kTableThreads));
+                                                           std::max(1ull, (run + ld::kTableThreads - 1) / ld::kTableThreads));
   blocks = std::min(blocks, max_blocks);
-  if (image > kMaxImage || blocks < 1) return ld_fail(LD_ERR_LIMIT, "matrix image exceeds the scratch array");
+  if (blocks < 1) return ld_fail(LD_ERR_LIMIT, "matrix image exceeds the scratch array");
 
   // upload image, built in a host stack buffer: header (counter 0, maximum
   // INT64_MIN), totals, initial H, packed rows
@@ -187,6 +223,10 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   pack_row(tot, C, W, PK, (uint32_t*)(img + kTot));
   pack_row(h0, C, W, PK, (uint32_t*)(img + kH0));
   for (int i = 0; i < R; ++i) pack_row(a + (size_t)i * C, C, W, PK, (uint32_t*)(img + kA) + (size_t)i * W);
+  if (P > 0) {
+    const ld_status sst = ld_sym_table(d, P, (uint64_t*)(img + sym_off));
+    if (sst != LD_OK) return sst;
+  }
   e = cudaMemcpyAsync(scratch, img, image, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return ld_fail(LD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
 
@@ -197,8 +237,10 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   args.tbias = nullptr;
   args.R = R; args.k = k; args.B = B; args.fw = fw;
   args.walk_len = walk_len; args.walk_begin = 0; args.walk_end = walks;
-  args.sym_digits = 0; args.sym_table = nullptr;   // every walk
-  args.rank_begin = args.rank_end = 0;
+  args.sym_digits = P;
+  args.sym_table = (const unsigned long long*)(scratch + sym_off);
+  args.rank_begin = 0;
+  args.rank_end = P > 0 ? run : 0;
   args.value_offset = offset;
   args.red.counter = (unsigned int*)(scratch + kCounter);
   args.red.gvalue = (long long*)(scratch + kGvalue);
@@ -215,7 +257,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   res->value = out.value;
   res->gray_index = out.index;
   res->labelings = walks * walk_len * (unsigned long long)B;
-  res->evaluated = res->labelings;
+  res->evaluated = run * walk_len * (unsigned long long)B;
   res->kernel_kind = LD_KERNEL_TABLE;
   res->lane_bits = 32 / PK;
   res->h2d_bytes = image;

@@ -21,6 +21,7 @@
 using namespace ldsolve;
 
 #include "../kernels/prune_kernel.cuh"
+#include "device_guard.h"
 
 namespace {
 
@@ -75,6 +76,7 @@ ld_status rest_norm(const int64_t* a, int C, int d, int marginal, int r, int dev
 extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int32_t d, int32_t marginal,
                                      const ld_options* opt, const int32_t* incumbent_labels,
                                      ld_result* res, int32_t* strategy, ld_prune_stats* stats) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!a || !res || R < 1 || C < 1) return ld_fail(LD_ERR_ARG, "bad arguments");
   ld_options o;
   if (opt) o = *opt; else ld_options_init(&o);

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "solver_internal.h"
+#include "device_guard.h"
 
 using namespace ldsolve;
 
@@ -69,6 +70,7 @@ bool checkpoint_write(const char* path, const Checkpoint& ck) {
 extern "C" ld_status ld_solve_resumable(const int64_t* a, int32_t rows, int32_t cols, int32_t d, int32_t marginal,
                                         const ld_options* opt, int32_t pieces, const char* checkpoint_path,
                                         int32_t max_pieces, int32_t* done, ld_result* res, int32_t* strategy) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!a || !checkpoint_path || !done || !res) return ld_fail(LD_ERR_ARG, "null argument");
   if (rows < 1 || cols < 1 || d < 1 || d > LD_MAX_D) return ld_fail(LD_ERR_ARG, "bad problem %d x %d, d=%d", rows, cols, d);
   if (pieces < 1) return ld_fail(LD_ERR_ARG, "pieces must be >= 1 (got %d)", pieces);

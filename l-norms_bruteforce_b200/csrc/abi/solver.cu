@@ -25,6 +25,7 @@
 #include "../kernels/registry.h"
 #include "../kernels/table_kernel.cuh"
 #include "../kernels/wide_kernel.cuh"
+#include "device_guard.h"
 
 using namespace ldsolve;
 
@@ -597,16 +598,19 @@ ld_status ldsolve::plan_fetch(ld_plan* p, ld_result* res, int32_t* strategy) {
 
 extern "C" ld_status ld_plan_create(const int64_t* a, int32_t rows, int32_t cols, int32_t d,
                                     int32_t marginal, const ld_options* opt, ld_plan** out) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!out) return ld_fail(LD_ERR_ARG, "null output");
   return plan_build(a, rows, cols, d, marginal, opt, nullptr, out);
 }
 
 extern "C" ld_status ld_plan_launch(ld_plan* plan) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!plan) return ld_fail(LD_ERR_ARG, "null plan");
   return plan_enqueue(plan);
 }
 
 extern "C" ld_status ld_plan_result(ld_plan* plan, ld_result* res, int32_t* strategy) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!plan || !res) return ld_fail(LD_ERR_ARG, "null argument");
   return plan_fetch(plan, res, strategy);
 }
@@ -644,11 +648,15 @@ extern "C" void* ld_plan_stream(const ld_plan* p) { return p && p->res ? (void*)
 
 extern "C" void* ld_plan_result_device(const ld_plan* p) { return p ? (void*)p->red.result : nullptr; }
 
-extern "C" void ld_plan_destroy(ld_plan* p) { plan_free(p); }
+extern "C" void ld_plan_destroy(ld_plan* p) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
+  plan_free(p);
+}
 
 extern "C" ld_status ld_solve_reduced(const int64_t* a, int32_t rows, int32_t cols, int32_t d,
                                       int32_t marginal, const ld_options* opt, ld_result* res,
                                       int32_t* strategy) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!res) return ld_fail(LD_ERR_ARG, "null result");
   const int dev = opt ? opt->device : 0;
   if (dev < 0 || dev >= 64) return ld_fail(LD_ERR_ARG, "device %d out of range", dev);

@@ -41,7 +41,10 @@ struct BatchArgs {
   Slot* chunk_results;      // one per chunk
 };
 
+// Threads per CTA: the autotuner picks 64, 128 or 256 per lane class (the
+// kernels read blockDim); 128 is the default.
 constexpr int kBatchThreads = 128;
+constexpr int kBatchMaxThreads = 256;
 
 // block-wide (max value, smallest index); the result is valid in thread 0
 __device__ __forceinline__ void block_best(long long& v, unsigned long long& n) {
@@ -120,7 +123,7 @@ __device__ __forceinline__ void batch_build_entry(int j, int k, const uint32_t* 
 }
 
 template <int D, int WB, int WA>
-__global__ void __launch_bounds__(kBatchThreads) batch_table_kernel(const BatchArgs args) {
+__global__ void __launch_bounds__(kBatchMaxThreads) batch_table_kernel(const BatchArgs args) {
   using S = Shape<D, WB, WA>;
   constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
   extern __shared__ __align__(16) uint32_t smem[];
@@ -261,7 +264,7 @@ __device__ __forceinline__ int scan_max_split(const uint32_t* H, const uint32_t*
 }
 
 template <int D, int WB>
-__global__ void __launch_bounds__(kBatchThreads) batch_split_kernel(const BatchArgs args) {
+__global__ void __launch_bounds__(kBatchMaxThreads) batch_split_kernel(const BatchArgs args) {
   static_assert(batch_split_class(WB, 0), "split classes: int32 words only, WB >= 40, a multiple of 8");
   constexpr int WH = WB / 2;
   using S = Shape<D, WH, 0>;

@@ -18,6 +18,7 @@
 
 #include "../abi/smem_limit.h"
 #include "../host/ld_internal.h"
+#include "../abi/device_guard.h"
 
 namespace {
 
@@ -141,6 +142,7 @@ size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 extern "C" ld_status ld_local_search(const int64_t* a, int32_t R, int32_t C, int32_t d, int32_t marginal,
                                      const int32_t* starts, int32_t n, int32_t max_rounds, int32_t device,
                                      int64_t* values, int32_t* labels) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!a || !starts || !values || !labels || n < 1 || R < 2 || C < 1)
     return ld_fail(LD_ERR_ARG, "bad local-search arguments");
   if (d < 1 || d > 3 || C > kLsMaxCols || R > kLsMaxRows)

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "../host/ld_internal.h"
+#include "../abi/device_guard.h"
 
 namespace {
 
@@ -30,6 +31,7 @@ __global__ void __launch_bounds__(256) int32_peak_kernel(int* sink, int iters, i
 
 // ops per launch = blocks * 256 threads * iters * 8 unroll * 8 chains * 2 ops
 extern "C" ld_status ld_measure_int32_peak(int32_t device, double* ops_per_second, double* ms) {
+  ldsolve::ContextRestore ctx_restore;   // the caller's current context, back on return
   if (!ops_per_second) return ld_fail(LD_ERR_ARG, "null output");
   if (cudaSetDevice(device) != cudaSuccess) return ld_fail(LD_ERR_NODEV, "no device %d", device);
   cudaDeviceProp p;

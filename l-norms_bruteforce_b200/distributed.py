@@ -27,17 +27,29 @@ def shard_bounds(units: int, index: int, count: int) -> tuple[int, int]:
     return lo, lo + q + (1 if index < r else 0)
 
 
-def combine(value: int, index: int, group=None, device=None) -> tuple[int, int]:
-    """Global (max value, smallest index attaining it) over the ranks."""
+def combine_tensor(val_idx, group=None):
+    """Global (max value, smallest index attaining it) of a 2-element int64
+    tensor (value, Gray index) per rank, without leaving the device: two
+    all-reduces (MAX on the value, MIN on the index of the ranks at the
+    maximum) queued on the current stream.  Returns two 1-element tensors.
+    Gray indices are below 2^63, so an index read as int64 keeps its order."""
     import torch
     import torch.distributed as dist
 
-    dev = device if device is not None else "cpu"
-    v = torch.tensor([value], dtype=torch.int64, device=dev)
+    v = val_idx[0:1].clone()
     dist.all_reduce(v, op=dist.ReduceOp.MAX, group=group)
-    mine = index if value == int(v.item()) else INT64_MAX
-    i = torch.tensor([mine], dtype=torch.int64, device=dev)
+    i = torch.where(val_idx[0:1] == v, val_idx[1:2], torch.full_like(val_idx[1:2], INT64_MAX))
     dist.all_reduce(i, op=dist.ReduceOp.MIN, group=group)
+    return v, i
+
+
+def combine(value: int, index: int, group=None, device=None) -> tuple[int, int]:
+    """Global (max value, smallest index attaining it) over the ranks, from
+    host integers (combine_tensor on a tensor of the given device)."""
+    import torch
+
+    dev = device if device is not None else "cpu"
+    v, i = combine_tensor(torch.tensor([value, index], dtype=torch.int64, device=dev), group=group)
     return int(v.item()), int(i.item())
 
 

@@ -7,7 +7,7 @@ reference's stdout and its strategy file.  The reference has no tests or
 fixtures of its own, so these outputs are what pins the oracle and the
 product.  Run from the repository root:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF_DIR=<reference checkout> && python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -72,7 +72,7 @@ def planted(rng: np.random.Generator, r: int, c: int, lo: int, hi: int) -> np.nd
 
 def main() -> None:
     if not REF.exists():
-        sys.exit("build the reference first: make -C oracle")
+        sys.exit("build the reference first: make -C oracle REF_DIR=<reference checkout>")
     rng = np.random.default_rng(20261203)
     cases = []
 

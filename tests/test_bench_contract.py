@@ -2,6 +2,7 @@
 from a plan description, the plain-method count, and the bounded CPU sample
 of a workload (no GPU needed)."""
 import importlib.util
+import json
 import sys
 from pathlib import Path
 
@@ -54,3 +55,54 @@ def test_clock_sampler_without_a_device(bench):
     c = bench.ClockSampler(0)
     out = c.stop()
     assert set(out) >= {"sm_mhz", "sm_max_mhz", "reasons"}
+
+
+def test_workload_config_is_the_libraries_reduction(bench, ld):
+    """The bench line's `config` (shared by both arms) names the reduced
+    shape and labeling count the library's preprocessing produces."""
+    for cfg in (1, 2, 3, 5):
+        inst = bench.instance(cfg)
+        c = bench.workload_config(inst)
+        info = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal).info
+        assert (c["rows"], c["cols"], c["labelings_per_step"]) == (info["rows"], info["cols"], info["labelings"])
+
+
+def test_reference_output_reduced_shape(bench, ld):
+    """The reference arm reads the reduced shape off the reference's own
+    stdout; on every golden case with a value line it equals the shape the
+    library's preprocessing leaves."""
+    import json
+    cases = json.loads((ROOT / "tests" / "golden" / "cases.json").read_text())
+    checked = 0
+    for case in cases:
+        if case["rc"] != 0 or " is: " not in case["stdout"] or "zero matrix" in case["stdout"]:
+            continue
+        value, rows, cols = bench.reference_output(case["stdout"])
+        tail = case["tail"]
+        d = int(tail[0])
+        stat = tail[1] if len(tail) > 1 and tail[1] not in ("m", "M") else "n"
+        marg = any(t in ("m", "M") for t in tail[1:]) and d == 1
+        p = ld.Problem.from_text(case["text"], d, stat, marg)
+        info = p.info
+        assert (rows, cols) == (info["rows"], info["cols"]), case["name"]
+        checked += 1
+    assert checked > 200
+
+
+def test_reference_arm_runs_the_full_file_without_the_library(tmp_path):
+    """`--impl reference` runs L_OpenMP on the whole input file with the
+    workload's flags and never maps liblnorms_b200.so into its process."""
+    import subprocess
+    if not (ROOT / "oracle" / "_ref" / "L_OpenMP").exists():
+        pytest.skip("reference binary not built")
+    code = ("import runpy, sys, json\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', '--config', '1']\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "print(json.dumps({'mapped': 'liblnorms_b200' in open('/proc/self/maps').read()}))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")]
+    line, mapped = lines[0], lines[1]
+    assert mapped == {"mapped": False}
+    assert line["impl"] == "reference" and line["config"]["labelings_per_step"] == 2 ** 23
+    assert line["details"]["reduced"] == [24, 24]

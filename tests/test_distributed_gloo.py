@@ -47,7 +47,13 @@ def _rank_main(rank, world, port, a, d, marg, shard_units, fail_rank, out):
             v, n = O.enumerate_max(a, d, marg, lo, hi, 1)
         else:
             v, n = np.iinfo(np.int64).min, np.iinfo(np.int64).max
-        out.put((rank, "ok", D.combine(int(v), int(n))))
+        host = D.combine(int(v), int(n))
+        # the tensor form bench.py queues on the solver's stream (same exchange)
+        import torch
+        tv, ti = D.combine_tensor(torch.tensor([int(v), int(n)], dtype=torch.int64))
+        if (int(tv.item()), int(ti.item())) != host:
+            raise AssertionError(f"combine_tensor {(int(tv.item()), int(ti.item()))} != combine {host}")
+        out.put((rank, "ok", host))
         dist.destroy_process_group()
     except Exception as e:   # reported to the parent
         out.put((rank, "error", repr(e)))
