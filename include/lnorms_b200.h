@@ -90,6 +90,14 @@ typedef struct {
                                    0 = the autotuner picks the column-split or
                                    the plain instance (plain when not tuned);
                                    1 = always column-split; -1 = never          */
+    int32_t column_split;       /* table kernel, one solve: lanes that share one
+                                   high index, each holding a slice of the
+                                   columns.  0 = only when the matrix is too
+                                   wide for one thread's registers (d <= 3:
+                                   > 64 int32 / > 128 8-bit columns; d >= 4:
+                                   > 16 / > 32); 2, 4 or 8 = that many lanes
+                                   whenever an instance fits; -1 = never (the
+                                   wide kernel takes wide matrices)            */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

@@ -23,6 +23,7 @@
 #include "smem_limit.h"
 #include "solver_internal.h"
 #include "../kernels/registry.h"
+#include "../kernels/split_kernel.cuh"
 #include "../kernels/table_kernel.cuh"
 #include "../kernels/wide_kernel.cuh"
 #include "device_guard.h"
@@ -101,6 +102,91 @@ bool table_config(const int64_t* a, int R, int C, int d, int marginal, int k, in
   return true;
 }
 
+// Bank padding of the column-split kernel's slice regions: the S lanes of a
+// group read, at step r of a tile, entry (g + r) mod S of slice g; with
+// 16-byte loads a quarter warp is served in one pass when those S addresses
+// fall on distinct groups of four banks.  Returns the padding (a multiple of
+// 4 words, below 32) with the fewest repeated bank groups over all r.
+int split_bank_pad(int S, int NW, int span) {
+  int best_pad = 0, best_cost = INT_MAX;
+  for (int pad = 0; pad < 32; pad += 4) {
+    int cost = 0;
+    for (int r = 0; r < S; ++r) {
+      int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int g = 0; g < S; ++g) cnt[((g * (span + pad) + ((g + r) % S) * NW) / 4) & 7]++;
+      for (int c : cnt) cost += c > 1 ? c - 1 : 0;
+    }
+    if (cost < best_cost) { best_cost = cost; best_pad = pad; }
+  }
+  return best_pad;
+}
+
+// The column-split form of the table kernel (split_kernel.cuh), for
+// matrices too wide for one thread's register vectors: over the low-row
+// counts k and the (S lanes, PW words) instances whose S x PW words hold a
+// row, the choice minimizing the table kernel's time estimate with the
+// ring's (2S - 1) instructions per labeling and the table padded to a
+// multiple of S entries.  Lanes: all 8-bit when every column passes
+// table_config's test, else all 32-bit.
+static bool split_choose(const int64_t* a, int R, int C, int d, int marginal, const ld_options& o,
+                         unsigned long long full_threads, Choice* ch) {
+  static const int kS[3] = {2, 4, 8}, kPW[3] = {8, 16, 32};
+  const int base = d <= 2 ? 2 : d, F = R - 1;
+  double best_t = 0;
+  bool found = false;
+  for (int k = 0; k <= F; ++k) {
+    const unsigned long long B = ipow(base, k);
+    if (B > 1024) break;
+    if (o.low_rows >= 0 && k != std::min(o.low_rows, F)) continue;
+    bool narrow = o.lane_bits != 32;
+    for (int l = 0; l < C && narrow; ++l) {
+      long long hb = 0, lb = 0;
+      for (int i = 0; i < R; ++i) {
+        const int64_t v = a[(size_t)i * C + l];
+        (i < k ? lb : hb) += v < 0 ? -(long long)v : (long long)v;
+      }
+      if (d == 1) narrow = (marginal && l == 0) ? (2 * hb <= 127 && 2 * lb <= 128) : (hb <= 127 && lb <= 127);
+      else narrow = hb + lb <= 127;
+    }
+    if (o.lane_bits == 8 && !narrow) continue;
+    const int PK = narrow ? 4 : 1;
+    const int wneed = PK == 4 ? (C + 3) / 4 : C;
+    double units = (double)ipow(base, F - k);
+    if (d >= 3 && !o.enumerate_all && F - k > 0) {
+      uint64_t pass = 0;
+      if (ld_symmetry_walks(d, F - k, 0, ipow(base, F - k), &pass) == LD_OK && pass > 0) units = (double)pass;
+    }
+    for (int S : kS) {
+      if (o.column_split > 0 && S != o.column_split) continue;
+      for (int PW : kPW) {
+        if (S * PW < wneed || !ld::table_split_kernel_ptr(d, PK, PW, S)) continue;
+        const int Wp = S * PW;
+        const unsigned long long Bp = (B + S - 1) / S * S;
+        if (Bp * (unsigned long long)(d * Wp) > (o.low_rows >= 0 ? 32768ull : 16384ull)) continue;
+        const double words = (double)d * Wp;
+        const double per_lab = (words + (2.0 * S - 1.0) / 2.0) * (double)Bp / (double)B + (2.0 * words + 40.0) / (double)B;
+        const double groups = (double)full_threads / S;
+        const double t = units * (double)B * per_lab / std::min(units, groups);
+        if (!found || t < best_t * 0.999) {
+          best_t = t;
+          found = true;
+          Choice c;
+          c.kind = LD_KERNEL_TABLE;
+          c.D = d; c.k = k; c.S = S; c.PW = PW; c.PK = PK;
+          c.WB = PK == 1 ? Wp : 0;
+          c.WA = PK == 4 ? Wp : 0;
+          c.WT = Wp;
+          c.order.clear();
+          for (int l = 0; l < C; ++l) c.order.push_back(l);
+          c.lane_bits = PK == 1 ? 32 : 8;
+          *ch = c;
+        }
+      }
+    }
+  }
+  return found;
+}
+
 // Pick the kernel and, for the table kernel, the low-row count minimizing
 // an estimate of the solve time: labelings x (words per labeling + the
 // amortized cost of a high-row step) / threads that have work.
@@ -112,11 +198,14 @@ ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, con
   const bool fits32 = vmax <= (long long)INT32_MAX && maxabs <= (long long)INT32_MAX;
   if (o.lane_bits && o.lane_bits != 8 && o.lane_bits != 32 && o.lane_bits != 64)
     return ld_fail(LD_ERR_ARG, "lane width %d is not 8, 32 or 64", o.lane_bits);
+  if (o.column_split != 0 && o.column_split != -1 && o.column_split != 2 && o.column_split != 4 &&
+      o.column_split != 8)
+    return ld_fail(LD_ERR_ARG, "column_split %d is not -1, 0, 2, 4 or 8", o.column_split);
   if (o.kernel != LD_KERNEL_WIDE && d <= 10 && o.lane_bits != 64 && fits32) {
     const int base = d <= 2 ? 2 : d, F = R - 1;
     double best_t = 0;
     bool found = false;
-    for (int k = 0; k <= F; ++k) {
+    for (int k = 0; k <= F && o.column_split <= 0; ++k) {
       const unsigned long long B = ipow(base, k);
       if (B > 1024) break;
       if (o.low_rows >= 0 && k != std::min(o.low_rows, F)) continue;
@@ -138,6 +227,10 @@ ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, con
       if (!found || t < best_t * 0.999) { best_t = t; *ch = c; found = true; }
     }
     if (found) return LD_OK;
+    // too wide for one thread's registers: S lanes share each high index
+    if (o.column_split >= 0 && split_choose(a, R, C, d, marginal, o, full_threads, ch)) return LD_OK;
+    if (o.column_split > 0)
+      return ld_fail(LD_ERR_ARG, "no column-split instance with %d lanes takes d=%d, %d columns", o.column_split, d, C);
     if (o.kernel == LD_KERNEL_TABLE)
       return ld_fail(LD_ERR_ARG, "the table kernel cannot take this matrix (d=%d, %d columns)", d, C);
   }
@@ -314,18 +407,28 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
   std::vector<char> image;
   if (p->ch.kind == LD_KERNEL_TABLE) {
     const int D = p->ch.D, WT = p->ch.WT;
-    p->kfn = ld::table_kernel_mixed_ptr(D, p->ch.WB, p->ch.WA);
-    if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no table kernel for D=%d WB=%d WA=%d", D, p->ch.WB, p->ch.WA); }
-    // LM with the marginal column in a 32-bit word of its own: its term is
-    // never negative, so the instance that adds it linearly applies
-    if (D == 1 && marginal && p->ch.WB >= 1 && !p->ch.order.empty() && p->ch.order[0] == 0) {
-      if (const void* lk = ld::table_kernel_lin_ptr(p->ch.WB, p->ch.WA)) { p->kfn = lk; p->ch.lin = 1; }
-    }
+    const int S = p->ch.S > 0 ? p->ch.S : 1;   // lanes per high index (column split)
     const int k = p->ch.k;
     p->k = k;
     p->B = (int)ipow(base, k);
     p->tpb = ld::kTableThreads;
-    p->smem = (size_t)ld::table_smem_words(D, WT, R, p->B) * sizeof(uint32_t);
+    if (p->ch.S > 0) {
+      p->kfn = ld::table_split_kernel_ptr(D, p->ch.PK, p->ch.PW, p->ch.S);
+      if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no column-split kernel for D=%d PW=%d S=%d", D, p->ch.PW, S); }
+      p->Bp = (p->B + S - 1) / S * S;
+      const int region = ld::split_region_words(D, p->ch.PW, R, p->Bp);
+      p->span = region + split_bank_pad(S, D * p->ch.PW, region);
+      p->smem = (size_t)S * p->span * sizeof(uint32_t);
+    } else {
+      p->kfn = ld::table_kernel_mixed_ptr(D, p->ch.WB, p->ch.WA);
+      if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no table kernel for D=%d WB=%d WA=%d", D, p->ch.WB, p->ch.WA); }
+      // LM with the marginal column in a 32-bit word of its own: its term is
+      // never negative, so the instance that adds it linearly applies
+      if (D == 1 && marginal && p->ch.WB >= 1 && !p->ch.order.empty() && p->ch.order[0] == 0) {
+        if (const void* lk = ld::table_kernel_lin_ptr(p->ch.WB, p->ch.WA)) { p->kfn = lk; p->ch.lin = 1; }
+      }
+      p->smem = (size_t)ld::table_smem_words(D, WT, R, p->B) * sizeof(uint32_t);
+    }
     if (ld_raise_smem_limit(p->kfn, p->smem) != cudaSuccess) {
       delete p; return ld_fail(LD_ERR_CUDA, "cannot reserve %zu bytes of shared memory", p->smem);
     }
@@ -333,7 +436,8 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, p->kfn, p->tpb, p->smem) != cudaSuccess || bps < 1) {
       delete p; return ld_fail(LD_ERR_CUDA, "table kernel does not fit an SM (smem %zu)", p->smem);
     }
-    const unsigned long long full = (unsigned long long)di.sms * bps * p->tpb;
+    // parallel units of a full grid: threads, or groups of S lanes
+    const unsigned long long full = (unsigned long long)di.sms * bps * (p->tpb / S);
     const int nh = F - k;
     // d >= 3: walks that hold no smallest index of a label-permutation
     // class are skipped (symmetry.c); the walks that run decide the length
@@ -372,12 +476,13 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
       p->rank_end = p->rank_begin + p->walks_run;
     }
     const unsigned long long mine = p->walks_run;
-    const unsigned long long want = (mine + p->tpb - 1) / p->tpb;
+    const unsigned long long per_block = (unsigned long long)(p->tpb / S);
+    const unsigned long long want = (mine + per_block - 1) / per_block;
     p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * bps, std::max(1ull, want));
     if (o.blocks > 0) p->blocks = o.blocks;
     // at least two walks per thread: the instance that walks two high
     // indices per thread against each table entry read (L_1 / LM, <= 10 words)
-    if (D == 1 && mine >= 2ull * (unsigned long long)p->blocks * (unsigned long long)p->tpb) {
+    if (D == 1 && p->ch.S == 0 && mine >= 2ull * (unsigned long long)p->blocks * (unsigned long long)p->tpb) {
       const void* pk = ld::table_kernel_pair_ptr(p->ch.WB, p->ch.WA, p->ch.lin);
       int pbps = 0;
       if (pk && ld_raise_smem_limit(pk, p->smem) == cudaSuccess &&
@@ -405,7 +510,14 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
         p->value_offset = kh + kl;
       }
     }
-    p->upload_bytes = kOffA + (size_t)R * WT * 4;
+    // vectors of up to 64 words sit at the fixed offsets; wider ones (column
+    // split) each take a multiple of 256 bytes
+    const size_t vec = std::max<size_t>(256, align256((size_t)WT * 4));
+    p->off_tot = kOffTot;
+    p->off_h0 = kOffTot + vec;
+    p->off_tb = kOffTot + 2 * vec;
+    p->off_A = kOffTot + 3 * vec;
+    p->upload_bytes = p->off_A + (size_t)R * WT * 4;
     if (p->sym_digits > 0) {   // completion counts for handing out walks by rank
       p->sym_off = align256(p->upload_bytes);
       p->upload_bytes = p->sym_off + ld_sym_table_len(d, p->sym_digits) * sizeof(uint64_t);
@@ -415,11 +527,11 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
       const ld_status sst = ld_sym_table(d, p->sym_digits, (uint64_t*)(image.data() + p->sym_off));
       if (sst != LD_OK) { delete p; return sst; }
     }
-    pack_row(tot.data(), p->ch, (uint32_t*)(image.data() + kOffTot));
-    pack_row(h0.data(), p->ch, (uint32_t*)(image.data() + kOffH0));
-    pack_row(tb.data(), p->ch, (uint32_t*)(image.data() + kOffTb));
+    pack_row(tot.data(), p->ch, (uint32_t*)(image.data() + p->off_tot));
+    pack_row(h0.data(), p->ch, (uint32_t*)(image.data() + p->off_h0));
+    pack_row(tb.data(), p->ch, (uint32_t*)(image.data() + p->off_tb));
     for (int i = 0; i < R; ++i)
-      pack_row(a + (size_t)i * C, p->ch, (uint32_t*)(image.data() + kOffA) + (size_t)i * WT);
+      pack_row(a + (size_t)i * C, p->ch, (uint32_t*)(image.data() + p->off_A) + (size_t)i * WT);
   } else {
     p->kfn = ld::wide_kernel_ptr(p->ch.i64, p->ch.PC, p->ch.multi, 0);
     if (!p->kfn) { delete p; return ld_fail(LD_ERR_ARG, "no wide kernel for PC=%d", p->ch.PC); }
@@ -521,10 +633,10 @@ ld_status ldsolve::plan_enqueue(ld_plan* p) {
   LD_CUDA(cudaEventRecord(r->ev0, r->stream));
   if (p->ch.kind == LD_KERNEL_TABLE) {
     ld::TableArgs args;
-    args.A = (const uint32_t*)(base_ptr + kOffA);
-    args.tot = (const uint32_t*)(base_ptr + kOffTot);
-    args.hinit = (const uint32_t*)(base_ptr + kOffH0);
-    args.tbias = (const uint32_t*)(base_ptr + kOffTb);
+    args.A = (const uint32_t*)(base_ptr + p->off_A);
+    args.tot = (const uint32_t*)(base_ptr + p->off_tot);
+    args.hinit = (const uint32_t*)(base_ptr + p->off_h0);
+    args.tbias = (const uint32_t*)(base_ptr + p->off_tb);
     args.R = p->R; args.k = p->k; args.B = p->B; args.fw = p->fw;
     args.walk_len = p->walk_len; args.walk_begin = p->walk_begin; args.walk_end = p->walk_end;
     args.sym_digits = p->sym_digits;
@@ -532,8 +644,18 @@ ld_status ldsolve::plan_enqueue(ld_plan* p) {
     args.rank_begin = p->rank_begin; args.rank_end = p->rank_end;
     args.value_offset = p->value_offset;
     args.red = p->red;
-    void* params[] = {&args};
-    LD_CUDA(cudaLaunchKernel(p->kfn, dim3(p->blocks), dim3(p->tpb), params, p->smem, r->stream));
+    if (p->ch.S > 0) {
+      ld::SplitArgs sargs;
+      sargs.t = args;
+      sargs.W = p->ch.WT;
+      sargs.Bp = p->Bp;
+      sargs.span = p->span;
+      void* params[] = {&sargs};
+      LD_CUDA(cudaLaunchKernel(p->kfn, dim3(p->blocks), dim3(p->tpb), params, p->smem, r->stream));
+    } else {
+      void* params[] = {&args};
+      LD_CUDA(cudaLaunchKernel(p->kfn, dim3(p->blocks), dim3(p->tpb), params, p->smem, r->stream));
+    }
   } else if (p->ch.i64) {
     ld::WideArgs<long long> args;
     args.A = (const long long*)(base_ptr + kOffA);
@@ -633,10 +755,10 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
              "table D=%d int32 words=%d int8x4 words=%d lin=%d pair=%d k=%d B=%d fw=%d walks=%llu run=%llu "
-             "sym=%d blocks=%d tpb=%d smem=%zu",
+             "sym=%d blocks=%d tpb=%d smem=%zu split=%d",
              p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->ch.pair, p->k, p->B, p->fw,
              (unsigned long long)p->walks, (unsigned long long)p->walks_run, p->sym_digits, p->blocks, p->tpb,
-             p->smem);
+             p->smem, p->ch.S);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d sym=%d walk_len=%llu run=%llu", p->ch.PC,
              p->ch.multi, p->ch.i64 ? "int64" : "int32", p->blocks, p->tpb, p->sym_digits,

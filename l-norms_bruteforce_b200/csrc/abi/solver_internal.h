@@ -42,6 +42,8 @@ struct Choice {
   int lane_bits = 0;
   int lin = 0;                                // table: LM column 0 linear in word 0
   int pair = 0;                               // table: two high indices per thread
+  int S = 0, PW = 0, PK = 0;                  // column-split table kernel: lanes per high
+                                              // index, words per lane, columns per word
 };
 
 inline int round4(int x) { return (x + 3) & ~3; }
@@ -53,6 +55,7 @@ inline unsigned long long ipow(unsigned long long b, int e) {
 }
 
 bool table_config(const int64_t* a, int R, int C, int d, int marginal, int k, int force_bits, Choice* ch);
+int split_bank_pad(int S, int NW, int span);
 ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, const Bounds& b,
                         const ld_options& o, unsigned long long full_threads, Choice* ch);
 void pack_row(const int64_t* row, const Choice& ch, uint32_t* out);
@@ -118,6 +121,9 @@ struct ld_plan {
   ldsolve::Resources own;
   ldsolve::Resources* res = nullptr;
   size_t upload_bytes = 0;
+  // table kernels: image offsets of the totals, initial H, table bias and rows
+  size_t off_tot = 0, off_h0 = 0, off_tb = 0, off_A = 0;
+  int Bp = 0, span = 0;                           // column split: table entries, words per slice region
   bool uploaded = false;       // the upload belongs to the next fetched launch
   ld::Reduce red{};
   const void* kfn = nullptr;

@@ -49,6 +49,17 @@ const void* batch_kernel_ptr(int D, int WB, int WA);
 // column-split instance of an int32 class (WB = 40, 48, 56, 64), or null
 const void* batch_split_kernel_ptr(int D, int WB);
 const void* batch_fold_kernel_ptr();
+// table_split_kernel<D, PK, PW, S> (split_kernel.cuh) by
+// [D][PK == 4][PW = 8, 16, 32][S = 2, 4, 8]: the column-split form of the
+// table kernel (S lanes per high index, PW words each); nullptr when not
+// instantiated.  Instances: split_d1.cu, split_d2.cu, split_d3.cu, split_dn.cu.
+using SplitKernelTab = const void* [11][2][3][3];
+void split_register_d1(SplitKernelTab& t);
+void split_register_d2(SplitKernelTab& t);
+void split_register_d3(SplitKernelTab& t);
+void split_register_d4_6(SplitKernelTab& t);
+void split_register_d7_10(SplitKernelTab& t);
+const void* table_split_kernel_ptr(int D, int PK, int PW, int S);
 // wide_kernel<IT, PC, MULTI>, PC in {1,2,4,...,128}
 // sym = 1: the instance that takes the walks passing the label-symmetry test by rank
 const void* wide_kernel_ptr(int i64, int PC, int multi, int sym);

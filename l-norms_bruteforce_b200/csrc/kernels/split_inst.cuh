@@ -1,0 +1,18 @@
+// Helpers that fill the column-split kernel lookup with instances.
+#pragma once
+#include "registry.h"
+#include "split_kernel.cuh"
+
+namespace ld {
+namespace inst {
+
+constexpr int split_pw_index(int PW) { return PW == 8 ? 0 : PW == 16 ? 1 : 2; }
+constexpr int split_s_index(int S) { return S == 2 ? 0 : S == 4 ? 1 : 2; }
+
+template <int D, int PK, int PW, int S>
+void split_put(SplitKernelTab& t) {
+  t[D][PK == 4 ? 1 : 0][split_pw_index(PW)][split_s_index(S)] = (const void*)&table_split_kernel<D, PK, PW, S>;
+}
+
+}  // namespace inst
+}  // namespace ld

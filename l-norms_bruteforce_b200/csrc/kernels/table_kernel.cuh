@@ -292,49 +292,54 @@ __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, i
   return m;
 }
 
-// D >= 4: tabulate, for every low labeling j (reflected base-D Gray word of
-// j), the vectors -L_1 .. -L_{D-1} (L_m: the low rows labelled m) and
-// T - (L_1 + .. + L_{D-1}).
+// D >= 4: table entry j (reflected base-D Gray word of j over the k low
+// rows) is the vectors -L_1 .. -L_{D-1} (L_m: the low rows labelled m) and
+// T - (L_1 + .. + L_{D-1}), written to e.
 template <int D, int WB, int WA>
-__device__ __forceinline__ void build_table_dn(const uint32_t* sA, const uint32_t* sTot, uint32_t* sT, int k, int B) {
+__device__ __forceinline__ void build_entry_dn(int j, const uint32_t* sA, const uint32_t* sTot, uint32_t* e,
+                                               int k) {
   using S = Shape<D, WB, WA>;
-  constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
-  for (int j = threadIdx.x; j < B; j += blockDim.x) {
-    uint32_t L[D - 1][WV];
+  constexpr int WT = S::WT, WV = S::WV;
+  uint32_t L[D - 1][WV];
+#pragma unroll
+  for (int v = 0; v < D - 1; ++v)
+#pragma unroll
+    for (int w = 0; w < WV; ++w) L[v][w] = 0u;
+  unsigned q = (unsigned)j;
+  for (int i = 0; i < k; ++i) {
+    const unsigned r = q % (2u * D);
+    const int lab = r < (unsigned)D ? (int)r : 2 * D - 1 - (int)r;
+    q /= (unsigned)D;
+    const uint32_t* row = sA + i * WT;
 #pragma unroll
     for (int v = 0; v < D - 1; ++v)
+      if (lab == v + 1) {
 #pragma unroll
-      for (int w = 0; w < WV; ++w) L[v][w] = 0u;
-    unsigned q = (unsigned)j;
-    for (int i = 0; i < k; ++i) {
-      const unsigned r = q % (2u * D);
-      const int lab = r < (unsigned)D ? (int)r : 2 * D - 1 - (int)r;
-      q /= (unsigned)D;
-      const uint32_t* row = sA + i * WT;
-#pragma unroll
-      for (int v = 0; v < D - 1; ++v)
-        if (lab == v + 1) {
-#pragma unroll
-          for (int w = 0; w < WV; ++w) L[v][w] = wadd<WB>(w, L[v][w], row[w]);
-        }
-    }
-    uint32_t* e = sT + j * NW;
-#pragma unroll
-    for (int w = 0; w < WT; ++w) {
-      if (w < WV) {
-        uint32_t rest = sTot[w];
-#pragma unroll
-        for (int v = 0; v < D - 1; ++v) {
-          e[v * WT + w] = wsub<WB>(w, 0u, L[v][w]);
-          rest = wsub<WB>(w, rest, L[v][w]);
-        }
-        e[(D - 1) * WT + w] = rest;
-      } else {
-#pragma unroll
-        for (int v = 0; v < D; ++v) e[v * WT + w] = 0u;
+        for (int w = 0; w < WV; ++w) L[v][w] = wadd<WB>(w, L[v][w], row[w]);
       }
+  }
+#pragma unroll
+  for (int w = 0; w < WT; ++w) {
+    if (w < WV) {
+      uint32_t rest = sTot[w];
+#pragma unroll
+      for (int v = 0; v < D - 1; ++v) {
+        e[v * WT + w] = wsub<WB>(w, 0u, L[v][w]);
+        rest = wsub<WB>(w, rest, L[v][w]);
+      }
+      e[(D - 1) * WT + w] = rest;
+    } else {
+#pragma unroll
+      for (int v = 0; v < D; ++v) e[v * WT + w] = 0u;
     }
   }
+}
+
+// D >= 4: every entry of the table, one thread per entry.
+template <int D, int WB, int WA>
+__device__ __forceinline__ void build_table_dn(const uint32_t* sA, const uint32_t* sTot, uint32_t* sT, int k, int B) {
+  for (int j = threadIdx.x; j < B; j += blockDim.x)
+    build_entry_dn<D, WB, WA>(j, sA, sTot, sT + j * Shape<D, WB, WA>::NW, k);
 }
 
 // PAIR instances (L_1 / LM, at most 10 words) walk two high indices per
@@ -436,6 +441,40 @@ __device__ __forceinline__ unsigned long long walk_of_rank(unsigned long long i,
   }
   for (int t = 0; t <= q; ++t) w *= (unsigned long long)D;
   return w + i;
+}
+
+// One step of a walk of high indices h0, h0 + 1, .. (h0 = wk * walk length,
+// a multiple of the walk length): from h - 1 to h (u = h - h0 > 0) high row
+// i moves from label a to label b.
+template <int D>
+__device__ __forceinline__ void high_step(unsigned long long wk, unsigned long long h, unsigned long long u,
+                                          int& i, int& a, int& b) {
+  if (D <= 2) {
+    i = __ffsll((long long)u) - 1;            // == ctz(h): h0 is a multiple of 2^fw
+    b = (int)(((h >> (i + 1)) & 1ull) ^ 1ull);
+    a = b ^ 1;
+  } else if (D >= 4) {
+    // digit i (the lowest nonzero base-D digit of u) steps from c - 1
+    // to c; its label is mirrored when h / D^(i+1) is odd
+    unsigned long long q = u;
+    i = 0;
+    while (q % (unsigned long long)D == 0ull) { q /= (unsigned long long)D; ++i; }
+    const int c = (int)(q % (unsigned long long)D);
+    unsigned long long hh = h;
+    for (int t = 0; t <= i; ++t) hh /= (unsigned long long)D;
+    const int par = (int)(hh & 1ull);
+    b = par ? D - 1 - c : c;
+    a = par ? D - c : c - 1;
+  } else {
+    unsigned long long q = u;
+    i = 0;
+    while (q % 3ull == 0ull) { q /= 3ull; ++i; }
+    const int c = (int)(q % 3ull);
+    // parity of h / 3^(i+1) = parity of wk (times an odd power) + u / 3^(i+1)
+    const int par = (int)((wk ^ (q / 3ull)) & 1ull);
+    b = par ? 2 - c : c;
+    a = par ? 3 - c : c - 1;
+  }
 }
 
 template <int D, int WB, int WA, bool LIN = false, bool PAIR = false>
@@ -565,34 +604,8 @@ __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(cons
     seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
     for (unsigned long long u = 0; u < WL; ++u) {
       if (u) {
-        const unsigned long long h = h0 + u;
         int i, a, b;
-        if (D <= 2) {
-          i = __ffsll((long long)u) - 1;            // == ctz(h): h0 is a multiple of 2^fw
-          b = (int)(((h >> (i + 1)) & 1ull) ^ 1ull);
-          a = b ^ 1;
-        } else if (D >= 4) {
-          // digit i (the lowest nonzero base-D digit of u) steps from c - 1
-          // to c; its label is mirrored when h / D^(i+1) is odd
-          unsigned long long q = u;
-          i = 0;
-          while (q % (unsigned long long)D == 0ull) { q /= (unsigned long long)D; ++i; }
-          const int c = (int)(q % (unsigned long long)D);
-          unsigned long long hh = h;
-          for (int t = 0; t <= i; ++t) hh /= (unsigned long long)D;
-          const int par = (int)(hh & 1ull);
-          b = par ? D - 1 - c : c;
-          a = par ? D - c : c - 1;
-        } else {
-          unsigned long long q = u;
-          i = 0;
-          while (q % 3ull == 0ull) { q /= 3ull; ++i; }
-          const int c = (int)(q % 3ull);
-          // parity of h / 3^(i+1) = parity of wk (times an odd power) + u / 3^(i+1)
-          const int par = (int)((wk ^ (q / 3ull)) & 1ull);
-          b = par ? 2 - c : c;
-          a = par ? 3 - c : c - 1;
-        }
+        high_step<D>(wk, h0 + u, u, i, a, b);
         move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
       }
       const int m = scan_max<D, WB, WA, LIN>(H, sT, B);

@@ -53,6 +53,23 @@ const void* table_kernel_ptr(int D, int W, int PK) {
   return nullptr;
 }
 
+const void* table_split_kernel_ptr(int D, int PK, int PW, int S) {
+  static SplitKernelTab tab = {};
+  static bool init = [] {
+    split_register_d1(tab);
+    split_register_d2(tab);
+    split_register_d3(tab);
+    split_register_d4_6(tab);
+    split_register_d7_10(tab);
+    return true;
+  }();
+  (void)init;
+  const int pi = PW == 8 ? 0 : PW == 16 ? 1 : PW == 32 ? 2 : -1;
+  const int si = S == 2 ? 0 : S == 4 ? 1 : S == 8 ? 2 : -1;
+  if (D < 1 || D > 10 || (PK != 1 && PK != 4) || pi < 0 || si < 0) return nullptr;
+  return tab[D][PK == 4 ? 1 : 0][pi][si];
+}
+
 static const PruneKernelTab& prune_kernels() {
   static PruneKernelTab tab = {};
   static bool init = [] {

@@ -1,0 +1,113 @@
+"""The column-split table kernel (split_kernel.cuh): matrices too wide for one
+thread's register vectors, where S lanes share each high index and hold a
+slice of the columns each.  Bit-exact against the oracle (value and smallest
+Gray index) at 65, 100, 200 and 256 columns for L_1, LM, d = 2, 3, 4 in
+32-bit and 8-bit lanes; every group size forced on the same matrices; label
+symmetry, shards and ties; and the wide kernel (column_split = -1) agrees."""
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+
+pytestmark = pytest.mark.gpu
+
+# rows per d: few enough that the oracle enumerates in well under a second
+ROWS = {1: 15, 2: 14, 3: 9, 4: 8}
+
+
+def _matrix(rng, d, cols, narrow):
+    r = ROWS[d]
+    amp = 3 if narrow else 400
+    if narrow and d >= 2:
+        amp = 1            # d >= 2 needs the full column sum within 8 bits
+    return rng.integers(-amp, amp + 1, size=(r, cols)).astype(np.int64)
+
+
+def _split_of(ld, a, d, marg, **kw):
+    plan = ld.Plan(a, d, marg, ld.options(**kw))
+    desc = plan.describe()
+    sol = plan.solve()
+    plan.close()
+    return sol, desc
+
+
+@pytest.mark.parametrize("cols", [65, 100, 200, 256])
+@pytest.mark.parametrize("kind", ["L1", "LM", "d2", "d3", "d4"])
+@pytest.mark.parametrize("narrow", [False, True], ids=["int32", "int8"])
+def test_wide_matrices_match_the_oracle(ld, kind, cols, narrow):
+    d = {"L1": 1, "LM": 1, "d2": 2, "d3": 3, "d4": 4}[kind]
+    marg = kind == "LM"
+    rng = np.random.default_rng(cols * 7 + d + 100 * marg + 1000 * narrow)
+    a = _matrix(rng, d, cols, narrow)
+    if marg:
+        a[-1, :] = rng.integers(-3, 4, size=cols)       # the marginal row
+        a[:, 0] = rng.integers(-3, 4, size=a.shape[0])  # the marginal column
+    sol, desc = _split_of(ld, a, d, marg)
+    # the unsplit kernel holds up to 64 int32 / 32 8-bit words per vector
+    # for d <= 3, 16 / 8 for d >= 4
+    words = (cols + 3) // 4 if narrow else cols
+    limit = (32 if narrow else 64) if d <= 3 else (8 if narrow else 16)
+    assert sol.kernel_kind == ld.KERNEL_TABLE, desc
+    assert (" split=0" not in desc) == (words > limit), desc
+    assert (sol.value, sol.gray_index) == O.enumerate_max(a, d, marg), desc
+    assert sol.lane_bits == (8 if narrow else 32), desc
+
+
+@pytest.mark.parametrize("S", [2, 4, 8])
+@pytest.mark.parametrize("d", [1, 2, 3, 4, 6, 10])
+def test_every_group_size_on_the_same_matrix(ld, S, d):
+    """Forced group sizes, including matrices the unsplit kernel also takes."""
+    rng = np.random.default_rng(10 * S + d)
+    rows = {1: 14, 2: 13, 3: 9, 4: 8, 6: 7, 10: 6}[d]
+    cols = {1: 40, 2: 30, 3: 24, 4: 20, 6: 12, 10: 8}[d]
+    a = rng.integers(-50, 51, size=(rows, cols)).astype(np.int64)
+    ref = O.enumerate_max(a, d, False)
+    sol, desc = _split_of(ld, a, d, False, column_split=S)
+    assert f" split={S}" in desc, desc
+    assert (sol.value, sol.gray_index) == ref, desc
+
+
+@pytest.mark.parametrize("d", [3, 4, 5])
+def test_label_symmetry_and_every_walk(ld, d):
+    rng = np.random.default_rng(70 + d)
+    a = rng.integers(-30, 31, size=({3: 10, 4: 8, 5: 7}[d], 120)).astype(np.int64)
+    ref = O.enumerate_max(a, d, False)
+    sym, desc = _split_of(ld, a, d, False, column_split=8)
+    full, _ = _split_of(ld, a, d, False, column_split=8, enumerate_all=1)
+    assert (sym.value, sym.gray_index) == ref == (full.value, full.gray_index), desc
+    assert sym.evaluated < full.evaluated == full.labelings
+
+
+@pytest.mark.parametrize("d", [1, 3])
+def test_shards_combine_to_the_oracle(ld, d):
+    rng = np.random.default_rng(5 + d)
+    a = rng.integers(-200, 201, size=({1: 16, 3: 10}[d], 150)).astype(np.int64)
+    ref = O.enumerate_max(a, d, False)
+    best = None
+    for i in range(3):
+        sol, desc = _split_of(ld, a, d, False, shard_index=i, shard_count=3)
+        assert " split=0" not in desc
+        cand = (sol.value, -sol.gray_index)
+        best = cand if best is None or cand > best else best
+    assert (best[0], -best[1]) == ref
+
+
+def test_ties_keep_the_smallest_index(ld):
+    a = np.ones((13, 130), dtype=np.int64)
+    a[1::2] *= -1
+    a[:, 64:] *= 2
+    for d in (1, 2, 3):
+        rr = a[: {1: 13, 2: 12, 3: 8}[d]]
+        sol, desc = _split_of(ld, rr, d, False)
+        assert " split=0" not in desc
+        assert (sol.value, sol.gray_index) == O.enumerate_max(rr, d, False), (d, desc)
+
+
+def test_wide_kernel_agrees(ld):
+    rng = np.random.default_rng(9)
+    for d, rows in ((1, 14), (2, 12), (3, 8)):
+        a = rng.integers(-99, 100, size=(rows, 180)).astype(np.int64)
+        split, desc = _split_of(ld, a, d, False)
+        wide, wdesc = _split_of(ld, a, d, False, column_split=-1)
+        assert " split=0" not in desc and wdesc.startswith("wide")
+        assert (split.value, split.gray_index) == (wide.value, wide.gray_index)
