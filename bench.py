@@ -666,10 +666,14 @@ def config5_leg(ld, local: int, count: int, steps: int, warmup: int) -> dict:
 def run_batch(args) -> None:
     """The 4096-matrix batch (n in [16, 32], m in [16, 64], d in {1, 2, 3}):
     one step = one replay of the batch's CUDA graph (persistent kernels per
-    lane class over a device work queue).  d = 3 matrices with more than
-    3^20 labelings are left out and reported: their ~2.2e16 labelings are
-    beyond any exhaustive enumeration.  value = labelings of the solved
-    matrices per second of device time."""
+    lane class over a device work queue).  The d = 3 matrices with more than
+    3^20 labelings (the tail: about 2.2e16 labelings, 251 matrices) stay out
+    of the replay.  value = labelings of the replayed matrices per second of
+    device time.  Outside the timed region every replayed result is checked
+    against a single solve (ld_solve_reduced) of the same matrix, and with
+    --tail-rows N every tail matrix of at most N rows is solved exactly, one
+    solve each; the rest of the tail is listed with its labelings and the
+    time the measured d = 3 rate gives it."""
     import torch
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -677,14 +681,14 @@ def run_batch(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(local)
     ld = load_package()
-    import lnorms_b200.workloads as W
-    mats, ds, skipped, skipped_lab, total, slots = [], [], 0, 0, 0, 0
-    for inst in W.config4()[: args.batch_count or None]:
+    W = load_workloads()
+    mats, ds, total, slots = [], [], 0, 0
+    tail = []   # (index in the workload, reduced matrix, labelings)
+    for idx, inst in enumerate(W.config4()[: args.batch_count or None]):
         p = ld.Problem.from_matrix(inst.matrix, inst.d)
         info = p.info
         if info["d"] == 3 and info["labelings"] > 3 ** 20:
-            skipped += 1
-            skipped_lab += int(info["labelings"])
+            tail.append((idx, p.reduced, int(info["labelings"])))
             continue
         mats.append(p.reduced)
         ds.append(info["d"])
@@ -720,6 +724,45 @@ def run_batch(args) -> None:
         bb.close()
         e2e.append(time.perf_counter() - t0)
         assert np.array_equal(ve, v0)
+    # full-scale check: every replayed result against a single solve
+    t0 = time.perf_counter()
+    bad = []
+    for i, (m, dd) in enumerate(zip(mats, ds)):
+        sol = ld.solve_reduced(m, dd, False, ld.options(device=local))
+        if (sol.value, sol.gray_index) != (int(v0[i]), int(g0[i])):
+            bad.append(i)
+    check_s = time.perf_counter() - t0
+    if bad:
+        raise AssertionError(f"{len(bad)} batch results differ from single solves, first {bad[:5]}")
+    # the d = 3 tail: exact single solves up to --tail-rows rows
+    tail_out = None
+    if tail:
+        solved, rest = [], []
+        for idx, m, lab in sorted(tail, key=lambda x: x[2]):
+            if m.shape[0] <= args.tail_rows:
+                t0 = time.perf_counter()
+                sol = ld.solve_reduced(m, 3, False, ld.options(device=local))
+                solved.append({"index": idx, "rows": m.shape[0], "cols": m.shape[1], "labelings": lab,
+                               "value": sol.value, "gray_index": sol.gray_index, "kernel_ms": sol.kernel_ms,
+                               "wall_s": time.perf_counter() - t0})
+            else:
+                rest.append({"index": idx, "rows": m.shape[0], "cols": m.shape[1], "labelings": lab})
+        rate = (sum(x["labelings"] for x in solved) / max(1e-9, sum(x["kernel_ms"] for x in solved) * 1e-3)
+                if solved else None)
+        if rate:   # cost of each remaining matrix at the measured rate, scaled by columns
+            mean_cols = sum(x["cols"] for x in solved) / len(solved)
+            for x in rest:
+                x["est_s"] = x["labelings"] / rate * (x["cols"] / mean_cols)
+        tail_out = {"matrices": len(tail), "labelings": sum(x[2] for x in tail),
+                    "solved": len(solved), "solved_labelings": sum(x["labelings"] for x in solved),
+                    "solved_kernel_s": sum(x["kernel_ms"] for x in solved) * 1e-3,
+                    "solved_wall_s": sum(x["wall_s"] for x in solved),
+                    "rate_labelings_per_s": rate, "max_rows_solved": args.tail_rows,
+                    "remaining": len(rest), "remaining_labelings": sum(x["labelings"] for x in rest),
+                    "remaining_est_s": sum(x.get("est_s", 0.0) for x in rest)}
+        if args.tail_out:
+            Path(args.tail_out).write_text(json.dumps({"summary": tail_out, "solved": solved, "remaining": rest},
+                                                      indent=1))
     if rank != 0:
         return
     dev_s = sum(ms) * 1e-3
@@ -733,10 +776,12 @@ def run_batch(args) -> None:
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator of the configuration)",
         "config": {"workload": f"config4: {len(mats)} of {args.batch_count or 4096} matrices, {total} labelings",
                    "matrices": len(mats), "labelings_per_step": total, "evaluated_per_step": n_eval,
-                   "skipped": {"matrices": skipped, "labelings": skipped_lab,
-                               "why": "d = 3 with more than 3^20 labelings"},
+                   "tail": {"matrices": len(tail), "labelings": sum(x[2] for x in tail),
+                            "why": "d = 3 with more than 3^20 labelings: solved one by one outside the replay"},
                    "batch": desc, "create_s": create_s,
                    "l2": "not flushed: the batch's inputs are a few MB and stay resident"},
+        "checked_against_single_solves": {"matrices": len(mats), "mismatches": 0, "s": check_s},
+        "tail": tail_out,
         "e2e": {"value": total / statistics.mean(e2e), "unit": "labelings/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": len(mats) * 16, "s_per_step": statistics.mean(e2e)},
         "roofline": {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "Tops/s",
@@ -890,6 +935,9 @@ def main() -> None:
     ap.add_argument("--batch-split", type=int, default=0, choices=(-1, 0, 1),
                     help="config 4: column-split instances of the wide int32 classes "
                          "(0 = the autotuner picks, 1 = always, -1 = never)")
+    ap.add_argument("--tail-rows", type=int, default=0,
+                    help="config 4: also solve the d = 3 tail matrices of at most this many rows, one by one")
+    ap.add_argument("--tail-out", default="", help="config 4: write the tail's per-matrix results to this JSON file")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")
     ap.add_argument("--ref-launch", default="",

@@ -98,6 +98,9 @@ typedef struct {
                                    > 16 / > 32); 2, 4 or 8 = that many lanes
                                    whenever an instance fits; -1 = never (the
                                    wide kernel takes wide matrices)            */
+    int32_t paired_walks;       /* table kernel, d <= 3: 0 = two high indices per
+                                   thread against each table read when every
+                                   thread has at least two walks; -1 = one   */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

@@ -481,9 +481,11 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
     p->blocks = (int)std::min<unsigned long long>((unsigned long long)di.sms * bps, std::max(1ull, want));
     if (o.blocks > 0) p->blocks = o.blocks;
     // at least two walks per thread: the instance that walks two high
-    // indices per thread against each table entry read (L_1 / LM, <= 10 words)
-    if (D == 1 && p->ch.S == 0 && mine >= 2ull * (unsigned long long)p->blocks * (unsigned long long)p->tpb) {
-      const void* pk = ld::table_kernel_pair_ptr(p->ch.WB, p->ch.WA, p->ch.lin);
+    // indices per thread against each table entry read (L_1 / LM, <= 10
+    // words; d = 2, 3, <= 8 words per vector)
+    if (D <= 3 && p->ch.S == 0 && o.paired_walks >= 0 &&
+        mine >= 2ull * (unsigned long long)p->blocks * (unsigned long long)p->tpb) {
+      const void* pk = ld::table_kernel_pair_ptr(D, p->ch.WB, p->ch.WA, p->ch.lin);
       int pbps = 0;
       if (pk && ld_raise_smem_limit(pk, p->smem) == cudaSuccess &&
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pbps, pk, p->tpb, p->smem) == cudaSuccess && pbps >= 1) {

@@ -27,10 +27,14 @@ void table_register_d1_lin(TableKernelLinTab& t);
 // (LIN only with WB in 1..2)
 using TableKernelPairTab = const void* [2][11][17];
 void table_register_pair(TableKernelPairTab& t);
+// table_kernel<D, WB, WA, false, PAIR = true> for D = 2, 3 by (D - 2, WB, WA):
+// WB in 1..8 with WA = 0, or WA in 1..8 with WB = 0
+using TableKernelPair23Tab = const void* [2][9][9];
+void table_register_pair23(TableKernelPair23Tab& t);
 
 // nullptr when not instantiated
 const void* table_kernel_mixed_ptr(int D, int WB, int WA);
-const void* table_kernel_pair_ptr(int WB, int WA, int lin);
+const void* table_kernel_pair_ptr(int D, int WB, int WA, int lin);
 const void* table_kernel_lin_ptr(int WB, int WA);
 // all columns in one lane width: PK = 1 (int32, W words) or 4 (int8x4, W words)
 const void* table_kernel_ptr(int D, int W, int PK);

@@ -342,10 +342,13 @@ __device__ __forceinline__ void build_table_dn(const uint32_t* sA, const uint32_
     build_entry_dn<D, WB, WA>(j, sA, sTot, sT + j * Shape<D, WB, WA>::NW, k);
 }
 
-// PAIR instances (L_1 / LM, at most 10 words) walk two high indices per
-// thread against each table entry read, within 64 registers so that 8
-// blocks stay resident per SM; the host uses them when a launch has at
+// PAIR instances walk two high indices per thread against each table entry
+// read: L_1 / LM with at most 10 words, within 64 registers so that 8
+// blocks stay resident per SM; d = 2 and 3 with at most 8 words per vector,
+// within 102 registers (5 blocks).  The host uses them when a launch has at
 // least two walks per thread.
+template <int D, bool PAIR>
+constexpr int table_min_blocks() { return PAIR ? (D == 1 ? 8 : 5) : 1; }
 
 // max over all B table entries for two register vectors H and G (two high
 // indices) at once: each entry is read from shared memory once for both.
@@ -478,8 +481,9 @@ __device__ __forceinline__ void high_step(unsigned long long wk, unsigned long l
 }
 
 template <int D, int WB, int WA, bool LIN = false, bool PAIR = false>
-__global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(const TableArgs args) {
-  static_assert(!PAIR || (D == 1 && WB + WA <= 10), "paired walks: L_1 / LM with at most 10 words");
+__global__ void __launch_bounds__(kTableThreads, (table_min_blocks<D, PAIR>())) table_kernel(const TableArgs args) {
+  static_assert(!PAIR || (D == 1 && WB + WA <= 10) || ((D == 2 || D == 3) && WB + WA <= 8),
+                "paired walks: L_1 / LM with at most 10 words, d = 2, 3 with at most 8");
   using S = Shape<D, WB, WA>;
   constexpr int WT = S::WT, WV = S::WV, NW = S::NW;
   extern __shared__ __align__(16) uint32_t smem[];
@@ -570,19 +574,31 @@ __global__ void __launch_bounds__(kTableThreads, PAIR ? 8 : 1) table_kernel(cons
   // per thread: both change the same row at each step (the step depends on
   // the offset u only), each in its own direction.
   if constexpr (PAIR) {
-    uint32_t G[WV];
-    for (unsigned long long wk = args.walk_begin + tid; wk < args.walk_end; wk += 2 * T) {
-      const unsigned long long h0 = wk * WL;
-      const unsigned long long g0 = (wk + T < args.walk_end ? wk + T : wk) * WL;   // a lone walk runs twice
+    uint32_t G[S::NR * WV];
+    // d = 3 with label symmetry: the passing walks, handed out by rank
+    const bool by_rank = D >= 3 && args.sym_digits > 0;
+    const unsigned long long it_end = by_rank ? args.rank_end : args.walk_end;
+    for (unsigned long long it = (by_rank ? args.rank_begin : args.walk_begin) + tid; it < it_end; it += 2 * T) {
+      const unsigned long long ig = it + T < it_end ? it + T : it;   // a lone walk runs twice
+      unsigned long long wk = it, wg = ig;
+      if constexpr (D >= 3) {
+        if (by_rank) {
+          wk = walk_of_rank<D>(it, args.sym_digits, args.sym_table);
+          wg = walk_of_rank<D>(ig, args.sym_digits, args.sym_table);
+        }
+      }
+      const unsigned long long h0 = wk * WL, g0 = wg * WL;
       seed_high<D, WB, WA>(H, sA, sH0, k, nh, h0);
       seed_high<D, WB, WA>(G, sA, sH0, k, nh, g0);
       for (unsigned long long u = 0; u < WL; ++u) {
         if (u) {
-          const int i = __ffsll((long long)u) - 1;
-          const int bh = (int)((((h0 + u) >> (i + 1)) & 1ull) ^ 1ull);
-          const int bg = (int)((((g0 + u) >> (i + 1)) & 1ull) ^ 1ull);
-          move_row<D, WB, WA>(H, sA + (k + i) * WT, bh ^ 1, bh);
-          move_row<D, WB, WA>(G, sA + (k + i) * WT, bg ^ 1, bg);
+          // both walks move the same row (the step depends on u only), each
+          // between its own labels
+          int i, a, b, ig2, ag, bg;
+          high_step<D>(wk, h0 + u, u, i, a, b);
+          high_step<D>(wg, g0 + u, u, ig2, ag, bg);
+          move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
+          move_row<D, WB, WA>(G, sA + (k + ig2) * WT, ag, bg);
         }
         int mh, mg;
         scan_max2<D, WB, WA, LIN>(H, G, sT, B, mh, mg);

@@ -36,14 +36,20 @@ const void* table_kernel_lin_ptr(int WB, int WA) {
   return tab[WB][WA];
 }
 
-const void* table_kernel_pair_ptr(int WB, int WA, int lin) {
+const void* table_kernel_pair_ptr(int D, int WB, int WA, int lin) {
   static TableKernelPairTab tab = {};
+  static TableKernelPair23Tab tab23 = {};
   static bool init = [] {
     table_register_pair(tab);
+    table_register_pair23(tab23);
     return true;
   }();
   (void)init;
-  if (WB < 0 || WB > 10 || WA < 0 || WA > 16 || WB + WA > 10) return nullptr;
+  if (D == 2 || D == 3) {
+    if (lin || WB < 0 || WB > 8 || WA < 0 || WA > 8) return nullptr;
+    return tab23[D - 2][WB][WA];
+  }
+  if (D != 1 || WB < 0 || WB > 10 || WA < 0 || WA > 16 || WB + WA > 10) return nullptr;
   return tab[lin ? 1 : 0][WB][WA];
 }
 

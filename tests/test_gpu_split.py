@@ -111,3 +111,35 @@ def test_wide_kernel_agrees(ld):
         wide, wdesc = _split_of(ld, a, d, False, column_split=-1)
         assert " split=0" not in desc and wdesc.startswith("wide")
         assert (split.value, split.gray_index) == (wide.value, wide.gray_index)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("blocks", [1, 2, 3])
+def test_paired_walks_match_single_walks_and_oracle(ld, d, blocks):
+    """Two high indices per thread against each table read (d = 1, 2, 3),
+    forced onto small matrices by a small grid; an odd walk count leaves one
+    thread a lone walk, which it runs twice."""
+    rng = np.random.default_rng(40 * d + blocks)
+    rows = {1: 17, 2: 16, 3: 11}[d]
+    for amp, cols in ((1, 30), (60, 20)):        # 8-bit and 32-bit lanes
+        a = rng.integers(-amp, amp + 1, size=(rows, cols)).astype(np.int64)
+        ref = O.enumerate_max(a, d, False)
+        # few low rows: thousands of walks, so even one block has two per thread
+        pair, desc = _split_of(ld, a, d, False, blocks=blocks, low_rows=3)
+        one, desc1 = _split_of(ld, a, d, False, blocks=blocks, low_rows=3, paired_walks=-1)
+        assert " pair=1" in desc and " pair=0" in desc1, (desc, desc1)
+        assert (pair.value, pair.gray_index) == ref == (one.value, one.gray_index), desc
+        assert pair.evaluated == one.evaluated
+
+
+def test_paired_walks_with_label_symmetry_and_shards(ld):
+    rng = np.random.default_rng(77)
+    a = rng.integers(-9, 10, size=(12, 24)).astype(np.int64)
+    ref = O.enumerate_max(a, 3, False)
+    best = None
+    for i in range(2):
+        sol, desc = _split_of(ld, a, 3, False, blocks=2, low_rows=2, shard_index=i, shard_count=2)
+        assert " pair=1" in desc and " sym=0" not in desc, desc
+        cand = (sol.value, -sol.gray_index)
+        best = cand if best is None or cand > best else best
+    assert (best[0], -best[1]) == ref
