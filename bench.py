@@ -693,7 +693,7 @@ def run_batch(args) -> None:
         mats.append(p.reduced)
         ds.append(info["d"])
         total += int(info["labelings"])
-    opts = ld.options(device=local, batch_split=args.batch_split)
+    opts = ld.options(device=local, batch_split=args.batch_split, threads_per_block=args.batch_tpb)
     t0 = time.perf_counter()
     b = ld.Batch(mats, ds, opts=opts, autotune=True)
     create_s = time.perf_counter() - t0
@@ -935,6 +935,8 @@ def main() -> None:
     ap.add_argument("--batch-split", type=int, default=0, choices=(-1, 0, 1),
                     help="config 4: column-split instances of the wide int32 classes "
                          "(0 = the autotuner picks, 1 = always, -1 = never)")
+    ap.add_argument("--batch-tpb", type=int, default=0, choices=(0, 64, 128, 256),
+                    help="config 4: threads per CTA of every lane class (0 = the autotuner picks)")
     ap.add_argument("--tail-rows", type=int, default=0,
                     help="config 4: also solve the d = 3 tail matrices of at most this many rows, one by one")
     ap.add_argument("--tail-out", default="", help="config 4: write the tail's per-matrix results to this JSON file")

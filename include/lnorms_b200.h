@@ -101,6 +101,9 @@ typedef struct {
     int32_t paired_walks;       /* table kernel, d <= 3: 0 = two high indices per
                                    thread against each table read when every
                                    thread has at least two walks; -1 = one   */
+    int32_t pack16;             /* table kernel: 0 = keep two running maxima in
+                                   one word (16 bits each) when every value is
+                                   below 65536; -1 = one maximum per word    */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

@@ -45,7 +45,8 @@ class Options(C.Structure):
                 ("blocks", C.c_int32), ("tile", C.c_int32), ("kernel", C.c_int32),
                 ("lane_bits", C.c_int32), ("shard_index", C.c_int32), ("shard_count", C.c_int32),
                 ("prune_policy", C.c_int32), ("enumerate_all", C.c_int32), ("batch_split", C.c_int32),
-                ("column_split", C.c_int32), ("paired_walks", C.c_int32), ("stream", C.c_void_p)]
+                ("column_split", C.c_int32), ("paired_walks", C.c_int32), ("pack16", C.c_int32),
+                ("stream", C.c_void_p)]
 
 
 class ProblemInfo(C.Structure):

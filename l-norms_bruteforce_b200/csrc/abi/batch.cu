@@ -436,10 +436,13 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     return LD_OK;
   };
   for (auto& c : b->classes) {
+    if (o.threads_per_block == 64 || o.threads_per_block == 128 || o.threads_per_block == 256)
+      c.tpb = o.threads_per_block;
     double mean = 0;
     for (int p : c.probs) mean += (double)walks[p];
     mean /= std::max<size_t>(1, c.probs.size());
-    const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)), (int)o.batch_split);
+    const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)),
+                                     (int)o.batch_split * 1000 + (int)o.threads_per_block);
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune.find(key);
@@ -455,9 +458,11 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     if (!autotune) continue;
     std::vector<Cand> cands;
     for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
-      for (int tpb : kTpbChoices)
+      for (int tpb : kTpbChoices) {
+        if (o.threads_per_block > 0 && tpb != o.threads_per_block) continue;   // forced block shape
         for (int wpt : {1, 2, 4, 8})
           for (double frac : {0.5, 1.0}) cands.push_back(Cand{variant, tpb, wpt, frac, 1e30f});
+      }
     for (auto& cd : cands) {
       st = time_cand(c, cd, 1, &cd.per);
       if (st != LD_OK) { batch_free(b); return st; }

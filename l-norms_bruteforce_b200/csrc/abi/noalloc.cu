@@ -242,6 +242,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   args.rank_begin = 0;
   args.rank_end = P > 0 ? run : 0;
   args.value_offset = offset;
+  args.pack16 = 0;
   args.red.counter = (unsigned int*)(scratch + kCounter);
   args.red.gvalue = (long long*)(scratch + kGvalue);
   args.red.result = (ld::Slot*)(scratch + kResult);

@@ -230,6 +230,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     t.sym_digits = (d == 3 && !o.enumerate_all && nh - fw > 0) ? nh - fw : 0;
     t.sym_table = nullptr; t.rank_begin = t.rank_end = 0;
     t.value_offset = offset;
+    t.pack16 = 0;
     t.red.counter = (unsigned int*)(dmem + 0);
     t.red.gvalue = (long long*)(dmem + 8);
     t.red.result = (ld::Slot*)(dmem + 16);

@@ -436,6 +436,7 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, p->kfn, p->tpb, p->smem) != cudaSuccess || bps < 1) {
       delete p; return ld_fail(LD_ERR_CUDA, "table kernel does not fit an SM (smem %zu)", p->smem);
     }
+    p->pack16 = (o.pack16 >= 0 && p->bounds.total + 2 * (marginal ? p->bounds.K : 0) < 65536) ? 1 : 0;
     // parallel units of a full grid: threads, or groups of S lanes
     const unsigned long long full = (unsigned long long)di.sms * bps * (p->tpb / S);
     const int nh = F - k;
@@ -645,6 +646,9 @@ ld_status ldsolve::plan_enqueue(ld_plan* p) {
     args.sym_table = (const unsigned long long*)(base_ptr + p->sym_off);
     args.rank_begin = p->rank_begin; args.rank_end = p->rank_end;
     args.value_offset = p->value_offset;
+    // every entry value in [0, 65536): the scans keep packed maxima (an
+    // entry's accumulator is at most sum |A| plus twice the LM shift)
+    args.pack16 = p->pack16;
     args.red = p->red;
     if (p->ch.S > 0) {
       ld::SplitArgs sargs;
@@ -757,10 +761,10 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
              "table D=%d int32 words=%d int8x4 words=%d lin=%d pair=%d k=%d B=%d fw=%d walks=%llu run=%llu "
-             "sym=%d blocks=%d tpb=%d smem=%zu split=%d",
+             "sym=%d blocks=%d tpb=%d smem=%zu split=%d p16=%d",
              p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->ch.pair, p->k, p->B, p->fw,
              (unsigned long long)p->walks, (unsigned long long)p->walks_run, p->sym_digits, p->blocks, p->tpb,
-             p->smem, p->ch.S);
+             p->smem, p->ch.S, p->pack16);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d sym=%d walk_len=%llu run=%llu", p->ch.PC,
              p->ch.multi, p->ch.i64 ? "int64" : "int32", p->blocks, p->tpb, p->sym_digits,

@@ -124,6 +124,7 @@ struct ld_plan {
   // table kernels: image offsets of the totals, initial H, table bias and rows
   size_t off_tot = 0, off_h0 = 0, off_tb = 0, off_A = 0;
   int Bp = 0, span = 0;                           // column split: table entries, words per slice region
+  int pack16 = 0;                                 // table kernel: packed 16-bit maxima
   bool uploaded = false;       // the upload belongs to the next fetched launch
   ld::Reduce red{};
   const void* kfn = nullptr;

@@ -62,6 +62,8 @@ struct TableArgs {
   const unsigned long long* sym_table;        // completion counts (walk_of_rank)
   unsigned long long rank_begin, rank_end;    // passing walks of this launch, by rank
   long long value_offset;   // subtracted from every value (LM shift K)
+  int pack16;               // every entry value lies in [0, 65536): maxima of two
+                            // values packed in one word (scan_max_p16, scan_max2_p16)
   Reduce red;
 };
 
@@ -290,6 +292,72 @@ __device__ __forceinline__ int scan_max(const uint32_t* H, const uint32_t* sT, i
   if (LIN && j > 0) m += (int)H[0];
   if (j < B) m = max(m, entry_value<D, WB, WA, LIN>(H, sT + j * S::NW));
   return m;
+}
+
+// Packed maxima.  When every value an entry can take lies in [0, 65536)
+// (the host checks sum |A| + K < 65536; all terms are absolute values, and
+// the LM linear column's term is never negative), two values share one word,
+// the second in the high half, formed by one multiply-add (off the integer
+// ALU pipe), and one 16-bit-pair max keeps both running maxima: one ALU
+// instruction per two labelings instead of two.  Entries of up to 32 words
+// are one accumulator chain each (two entries, or two high indices, give the
+// chains their independence); longer ones alternate two chains.
+
+// acc (+)= |H - e| over one entry, as one chain (NW <= 32) or two
+template <int D, int WB, int WA, bool LIN>
+__device__ __forceinline__ uint32_t entry_acc(const uint32_t* H, const uint4* t) {
+  using S = Shape<D, WB, WA>;
+  uint32_t a0 = 0u, a1 = 0u;
+  if constexpr (S::NW <= 32) {
+#pragma unroll
+    for (int q = 0; q < S::NW / 4; ++q) sad4<D, WB, WA, LIN>(H, t[q], q, a0, a0);
+    return a0;
+  } else {
+#pragma unroll
+    for (int q = 0; q < S::NW / 4; ++q) sad4<D, WB, WA, LIN>(H, t[q], q, a0, a1);
+    return a0 + a1;
+  }
+}
+
+// scan_max with packed maxima (TableArgs::pack16)
+template <int D, int WB, int WA, bool LIN = false>
+__device__ __forceinline__ int scan_max_p16(const uint32_t* H, const uint32_t* sT, int B) {
+  using S = Shape<D, WB, WA>;
+  uint32_t m = 0u;   // low half: even entries, high half: odd entries
+  int j = 0;
+  for (; j + 2 <= B; j += 2) {
+    const uint32_t a = entry_acc<D, WB, WA, LIN>(H, reinterpret_cast<const uint4*>(sT + j * S::NW));
+    const uint32_t b = entry_acc<D, WB, WA, LIN>(H, reinterpret_cast<const uint4*>(sT + (j + 1) * S::NW));
+    m = __vmaxu2(m, b * 65536u + a);
+  }
+  int r = max((int)(m & 0xffffu), (int)(m >> 16));
+  if (LIN) r += (int)H[0];
+  if (j < B) r = max(r, entry_value<D, WB, WA, LIN>(H, sT + j * S::NW));
+  return r;
+}
+
+// scan_max2 with packed maxima: H's value in the low half, G's in the high
+// half of each entry's word; two entries per step
+template <int D, int WB, int WA, bool LIN = false>
+__device__ __forceinline__ void scan_max2_p16(const uint32_t* H, const uint32_t* G, const uint32_t* sT, int B,
+                                              int& mh, int& mg) {
+  using S = Shape<D, WB, WA>;
+  uint32_t m = 0u;
+  int j = 0;
+  for (; j + 2 <= B; j += 2) {
+    const uint4* t0 = reinterpret_cast<const uint4*>(sT + j * S::NW);
+    const uint4* t1 = reinterpret_cast<const uint4*>(sT + (j + 1) * S::NW);
+    const uint32_t a0 = entry_acc<D, WB, WA, LIN>(H, t0), b0 = entry_acc<D, WB, WA, LIN>(G, t0);
+    const uint32_t a1 = entry_acc<D, WB, WA, LIN>(H, t1), b1 = entry_acc<D, WB, WA, LIN>(G, t1);
+    m = __vmaxu2(m, b0 * 65536u + a0);
+    m = __vmaxu2(m, b1 * 65536u + a1);
+  }
+  if (j < B) {
+    const uint4* t0 = reinterpret_cast<const uint4*>(sT + j * S::NW);
+    m = __vmaxu2(m, entry_acc<D, WB, WA, LIN>(G, t0) * 65536u + entry_acc<D, WB, WA, LIN>(H, t0));
+  }
+  mh = (int)(m & 0xffffu) + (LIN ? (int)H[0] : 0);
+  mg = (int)(m >> 16) + (LIN ? (int)G[0] : 0);
 }
 
 // D >= 4: table entry j (reflected base-D Gray word of j over the k low
@@ -601,7 +669,8 @@ __global__ void __launch_bounds__(kTableThreads, (table_min_blocks<D, PAIR>())) 
           move_row<D, WB, WA>(G, sA + (k + ig2) * WT, ag, bg);
         }
         int mh, mg;
-        scan_max2<D, WB, WA, LIN>(H, G, sT, B, mh, mg);
+        if (args.pack16) scan_max2_p16<D, WB, WA, LIN>(H, G, sT, B, mh, mg);
+        else scan_max2<D, WB, WA, LIN>(H, G, sT, B, mh, mg);
         // keep the smallest high index among equal maxima
         if (mh > best || (mh == best && h0 + u < best_h)) { best = mh; best_h = h0 + u; }
         if (mg > best || (mg == best && g0 + u < best_h)) { best = mg; best_h = g0 + u; }
@@ -624,7 +693,7 @@ __global__ void __launch_bounds__(kTableThreads, (table_min_blocks<D, PAIR>())) 
         high_step<D>(wk, h0 + u, u, i, a, b);
         move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
       }
-      const int m = scan_max<D, WB, WA, LIN>(H, sT, B);
+      const int m = args.pack16 ? scan_max_p16<D, WB, WA, LIN>(H, sT, B) : scan_max<D, WB, WA, LIN>(H, sT, B);
       if (m > best) { best = m; best_h = h0 + u; }
     }
   }

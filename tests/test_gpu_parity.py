@@ -280,7 +280,7 @@ def test_plans_sharing_a_kernel_keep_their_shared_memory(ld):
     pb = ld.Plan(small, 1)
     da, db = pa.describe(), pb.describe()
     assert da.split(" k=")[0] == db.split(" k=")[0]               # same instance
-    assert int(da.split("smem=")[1]) > int(db.split("smem=")[1])
+    assert int(da.split("smem=")[1].split()[0]) > int(db.split("smem=")[1].split()[0])
     sa = pa.solve()
     assert (sa.value, sa.gray_index) == O.enumerate_max(big, 1, False)
     sb = pb.solve()

@@ -121,7 +121,7 @@ def test_paired_walks_match_single_walks_and_oracle(ld, d, blocks):
     thread a lone walk, which it runs twice."""
     rng = np.random.default_rng(40 * d + blocks)
     rows = {1: 17, 2: 16, 3: 11}[d]
-    for amp, cols in ((1, 30), (60, 20)):        # 8-bit and 32-bit lanes
+    for amp, cols in ((1, 30), (60, 8)):         # 8-bit and 32-bit lanes (paired: <= 8 words)
         a = rng.integers(-amp, amp + 1, size=(rows, cols)).astype(np.int64)
         ref = O.enumerate_max(a, d, False)
         # few low rows: thousands of walks, so even one block has two per thread
@@ -143,3 +143,27 @@ def test_paired_walks_with_label_symmetry_and_shards(ld):
         cand = (sol.value, -sol.gray_index)
         best = cand if best is None or cand > best else best
     assert (best[0], -best[1]) == ref
+
+
+@pytest.mark.parametrize("d,marg", [(1, False), (1, True), (2, False), (3, False), (5, False)])
+def test_packed_maxima_at_the_16_bit_bound(ld, d, marg):
+    """Two running maxima per word (p16=1) whenever sum |A| + 2K < 65536:
+    totals just below the bound use it, just above do not, and both give the
+    oracle's answer; pack16 = -1 turns it off."""
+    rows = {1: 14, 2: 12, 3: 9, 5: 7}[d]
+    for total, want in ((65000, 1), (66500, 0)):
+        rng = np.random.default_rng(total + d)
+        a = rng.integers(1, 100, size=(rows, 12)).astype(np.int64) * rng.choice([-1, 1], size=(rows, 12))
+        if marg:
+            a[:, 0] = rng.integers(-3, 4, size=rows)
+        # scale column 1 so that sum |A| (+ 2K) lands on the target
+        k = int(np.abs(a[:, 0]).sum()) if marg else 0
+        rest = int(np.abs(a).sum() - np.abs(a[:, 1]).sum()) + 2 * k
+        a[:, 1] = np.sign(a[:, 1]) * ((total - rest) // rows)
+        a[0, 1] += np.sign(a[0, 1]) * ((total - rest) % rows)
+        assert int(np.abs(a).sum()) + 2 * k == total
+        ref = O.enumerate_max(a, d, marg)
+        sol, desc = _split_of(ld, a, d, marg)
+        off, desc_off = _split_of(ld, a, d, marg, pack16=-1)
+        assert f" p16={want}" in desc and " p16=0" in desc_off, (desc, desc_off)
+        assert (sol.value, sol.gray_index) == ref == (off.value, off.gray_index), desc
