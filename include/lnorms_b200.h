@@ -104,6 +104,9 @@ typedef struct {
     int32_t pack16;             /* table kernel: 0 = keep two running maxima in
                                    one word (16 bits each) when every value is
                                    below 65536; -1 = one maximum per word    */
+    int32_t walk_fetch;         /* table kernel: 0 = warps fetch walks from a
+                                   counter as they finish (balanced); -1 =
+                                   every thread takes a fixed share         */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

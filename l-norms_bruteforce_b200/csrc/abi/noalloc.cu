@@ -247,6 +247,7 @@ extern "C" ld_status ld_solve_reduced_noalloc(const int64_t* a, int32_t R, int32
   args.red.gvalue = (long long*)(scratch + kGvalue);
   args.red.result = (ld::Slot*)(scratch + kResult);
   args.red.slots = (ld::Slot*)(scratch + off_slots);
+  args.red.work = nullptr;   // walks split statically
   void* params[] = {&args};
   e = cudaLaunchKernel(kfn, dim3((unsigned)blocks), dim3(ld::kTableThreads), params, smem, st);
   if (e != cudaSuccess) return ld_fail(LD_ERR_CUDA, "launch: %s", cudaGetErrorString(e));

@@ -235,6 +235,7 @@ extern "C" ld_status ld_solve_pruned(const int64_t* a, int32_t R, int32_t C, int
     t.red.gvalue = (long long*)(dmem + 8);
     t.red.result = (ld::Slot*)(dmem + 16);
     t.red.slots = (ld::Slot*)(dmem + off_slots);
+    t.red.work = nullptr;
     args.ttop = (const uint32_t*)(dmem + offTtop);
     args.thigh = (const uint32_t*)(dmem + offThigh);
     args.threshold = thr;

@@ -619,6 +619,10 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
   p->red.gvalue = (long long*)(base_ptr + kOffGvalue);
   p->red.result = (ld::Slot*)(base_ptr + kOffResult);
   p->red.slots = (ld::Slot*)(base_ptr + off_slots);
+  // the table kernel's warps fetch walks from a counter in the header (zero
+  // in the upload image, reset by each launch's last block)
+  p->red.work = (p->ch.kind == LD_KERNEL_TABLE && p->ch.S == 0 && o.walk_fetch >= 0)
+                    ? (unsigned long long*)(base_ptr + kOffWork) : nullptr;
   memcpy(p->res->hstage, image.data(), p->upload_bytes);
   cudaError_t ce = cudaMemcpyAsync(p->res->dmem, p->res->hstage, p->upload_bytes, cudaMemcpyHostToDevice,
                                    p->res->stream);
@@ -761,10 +765,10 @@ extern "C" ld_status ld_plan_describe(const ld_plan* p, char* buf, size_t cap) {
   if (p->ch.kind == LD_KERNEL_TABLE)
     snprintf(buf, cap,
              "table D=%d int32 words=%d int8x4 words=%d lin=%d pair=%d k=%d B=%d fw=%d walks=%llu run=%llu "
-             "sym=%d blocks=%d tpb=%d smem=%zu split=%d p16=%d",
+             "sym=%d blocks=%d tpb=%d smem=%zu split=%d p16=%d fetch=%d",
              p->ch.D, p->ch.WB, p->ch.WA, p->ch.lin, p->ch.pair, p->k, p->B, p->fw,
              (unsigned long long)p->walks, (unsigned long long)p->walks_run, p->sym_digits, p->blocks, p->tpb,
-             p->smem, p->ch.S, p->pack16);
+             p->smem, p->ch.S, p->pack16, p->red.work ? 1 : 0);
   else
     snprintf(buf, cap, "wide PC=%d multi=%d %s blocks=%d tpb=%d sym=%d walk_len=%llu run=%llu", p->ch.PC,
              p->ch.multi, p->ch.i64 ? "int64" : "int32", p->blocks, p->tpb, p->sym_digits,

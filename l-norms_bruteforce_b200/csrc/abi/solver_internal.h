@@ -91,7 +91,7 @@ extern Resources g_pws[64];
 
 // a plan's device image: reduction header, then totals, initial H, table
 // bias and packed rows
-constexpr size_t kOffCounter = 0, kOffGvalue = 8, kOffResult = 16;
+constexpr size_t kOffCounter = 0, kOffGvalue = 8, kOffResult = 16, kOffWork = 32;
 constexpr size_t kOffTot = 256, kOffH0 = 512, kOffTb = 768, kOffA = 1024;
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }

@@ -23,6 +23,8 @@ struct Reduce {
   unsigned int* counter;
   long long* gvalue;
   Slot* result;
+  unsigned long long* work;   // walk counter the launch's warps fetch from (0 before
+                              // the launch, reset by the last block), or null
 };
 
 // ---- packed integer lanes ----------------------------------------------
@@ -117,6 +119,7 @@ __device__ __forceinline__ void grid_reduce(long long v, unsigned long long n, c
     R.result->index = best;
     *R.gvalue = LLONG_MIN;
     *R.counter = 0u;
+    if (R.work) *R.work = 0ull;   // every block has finished fetching walks
     __threadfence();
   }
 }

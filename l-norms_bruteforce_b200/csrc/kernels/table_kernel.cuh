@@ -641,13 +641,27 @@ __global__ void __launch_bounds__(kTableThreads, (table_min_blocks<D, PAIR>())) 
   // Two walks (wk and wk + T) in lockstep when there are at least two walks
   // per thread: both change the same row at each step (the step depends on
   // the offset u only), each in its own direction.
+  // d >= 3 with label symmetry: the passing walks, handed out by rank
+  const bool by_rank = D >= 3 && args.sym_digits > 0;
+  const unsigned long long it_begin = by_rank ? args.rank_begin : args.walk_begin;
+  const unsigned long long it_end = by_rank ? args.rank_end : args.walk_end;
+  // Walks go to threads statically (walk it_begin + tid, then every T-th),
+  // or, when the launch has a walk counter, 32 (paired: 64) at a time to a
+  // warp, so that threads that finish early take more: with a few walks per
+  // thread the static split leaves up to one walk (pair) per thread idle at
+  // the end.  Fetched walks need not come in increasing order, so every
+  // update keeps the smallest high index among equal maxima.
+  const int lane = threadIdx.x & 31;
+  unsigned long long fetched = 0ull;
+  auto fetch = [&](unsigned long long n) -> bool {   // warp-uniform; false when no walks are left
+    unsigned long long base = 0ull;
+    if (lane == 0) base = atomicAdd(args.red.work, n);
+    fetched = __shfl_sync(0xffffffffu, base, 0);
+    return it_begin + fetched < it_end;
+  };
   if constexpr (PAIR) {
     uint32_t G[S::NR * WV];
-    // d = 3 with label symmetry: the passing walks, handed out by rank
-    const bool by_rank = D >= 3 && args.sym_digits > 0;
-    const unsigned long long it_end = by_rank ? args.rank_end : args.walk_end;
-    for (unsigned long long it = (by_rank ? args.rank_begin : args.walk_begin) + tid; it < it_end; it += 2 * T) {
-      const unsigned long long ig = it + T < it_end ? it + T : it;   // a lone walk runs twice
+    auto run_pair = [&](unsigned long long it, unsigned long long ig) {
       unsigned long long wk = it, wg = ig;
       if constexpr (D >= 3) {
         if (by_rank) {
@@ -675,12 +689,18 @@ __global__ void __launch_bounds__(kTableThreads, (table_min_blocks<D, PAIR>())) 
         if (mh > best || (mh == best && h0 + u < best_h)) { best = mh; best_h = h0 + u; }
         if (mg > best || (mg == best && g0 + u < best_h)) { best = mg; best_h = g0 + u; }
       }
+    };
+    if (args.red.work) {
+      while (fetch(64ull)) {
+        const unsigned long long it = it_begin + fetched + lane, ig = it + 32ull;
+        if (it < it_end) run_pair(it, ig < it_end ? ig : it);   // a lone walk runs twice
+      }
+    } else {
+      for (unsigned long long it = it_begin + tid; it < it_end; it += 2 * T)
+        run_pair(it, it + T < it_end ? it + T : it);
     }
   } else {
-  // d >= 3 with label symmetry: the passing walks, handed out by rank
-  const bool by_rank = D >= 3 && args.sym_digits > 0;
-  const unsigned long long it_end = by_rank ? args.rank_end : args.walk_end;
-  for (unsigned long long it = (by_rank ? args.rank_begin : args.walk_begin) + tid; it < it_end; it += T) {
+  auto run_walk = [&](unsigned long long it) {
     unsigned long long wk = it;
     if constexpr (D >= 3) {
       if (by_rank) wk = walk_of_rank<D>(it, args.sym_digits, args.sym_table);
@@ -694,8 +714,16 @@ __global__ void __launch_bounds__(kTableThreads, (table_min_blocks<D, PAIR>())) 
         move_row<D, WB, WA>(H, sA + (k + i) * WT, a, b);
       }
       const int m = args.pack16 ? scan_max_p16<D, WB, WA, LIN>(H, sT, B) : scan_max<D, WB, WA, LIN>(H, sT, B);
-      if (m > best) { best = m; best_h = h0 + u; }
+      if (m > best || (m == best && h0 + u < best_h)) { best = m; best_h = h0 + u; }
     }
+  };
+  if (args.red.work) {
+    while (fetch(32ull)) {
+      const unsigned long long it = it_begin + fetched + lane;
+      if (it < it_end) run_walk(it);
+    }
+  } else {
+    for (unsigned long long it = it_begin + tid; it < it_end; it += T) run_walk(it);
   }
   }
 

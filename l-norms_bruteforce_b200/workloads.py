@@ -104,6 +104,17 @@ def config4(count: int = 4096, seed: int = 4,
     return out
 
 
+def wide(cols: int, d: int = 1, rows: int = 0, amp: int = 40, seed: int = 6) -> Instance:
+    """A matrix wider than one thread's register vectors hold (the
+    reference's CLI takes up to 4096 columns, functions.h:2): rows x cols
+    uniform integers in [-amp, amp] (32-bit lanes), no flag.  Default rows:
+    2^31 labelings for d <= 2, 3^20 for d = 3."""
+    rows = rows or {1: 32, 2: 32, 3: 21}.get(d, 12)
+    rng = np.random.default_rng(seed)
+    a = rng.integers(-amp, amp + 1, size=(rows, cols), dtype=np.int64)
+    return Instance(f"wide_L{d}_{rows}x{cols}", a, d=d)
+
+
 def lowrank(n: int, m: int, rng: np.random.Generator, rank: int = 3,
             scale: float = 5.0, noise: int = 2) -> np.ndarray:
     """round(scale * U V) + uniform integer noise in [-noise, noise]."""

@@ -106,3 +106,12 @@ def test_reference_arm_runs_the_full_file_without_the_library(tmp_path):
     assert mapped == {"mapped": False}
     assert line["impl"] == "reference" and line["config"]["labelings_per_step"] == 2 ** 23
     assert line["details"]["reduced"] == [24, 24]
+
+
+def test_issue_slots_of_the_column_split_count_real_columns(bench):
+    d = ("table D=1 int32 words=256 int8x4 words=0 lin=0 pair=0 k=6 B=64 fw=4 walks=1 run=1 sym=0 "
+         "blocks=1 tpb=128 smem=1 split=8 p16=0")
+    assert bench.issue_ops_per_labeling(d, 1, 200)[0] == 400
+    d = ("table D=3 int32 words=0 int8x4 words=64 lin=0 pair=0 k=3 B=27 fw=0 walks=1 run=1 sym=5 "
+         "blocks=1 tpb=128 smem=1 split=4 p16=1")
+    assert bench.issue_ops_per_labeling(d, 3, 250)[0] == 2 * 3 * 63

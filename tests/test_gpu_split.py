@@ -167,3 +167,24 @@ def test_packed_maxima_at_the_16_bit_bound(ld, d, marg):
         off, desc_off = _split_of(ld, a, d, marg, pack16=-1)
         assert f" p16={want}" in desc and " p16=0" in desc_off, (desc, desc_off)
         assert (sol.value, sol.gray_index) == ref == (off.value, off.gray_index), desc
+
+
+@pytest.mark.parametrize("d", [1, 2, 3, 4])
+def test_fetched_walks_match_the_static_split_on_every_launch(ld, d):
+    """Warps fetching walks from a counter (the default) against the fixed
+    split (walk_fetch = -1): the same answer as the oracle, launch after
+    launch of one plan (the last block resets the counter), with ties."""
+    rng = np.random.default_rng(90 + d)
+    rows = {1: 18, 2: 17, 3: 11, 4: 9}[d]
+    a = rng.integers(-2, 3, size=(rows, 9)).astype(np.int64)
+    a[1] = a[0]                               # equal rows: many tied labelings
+    ref = O.enumerate_max(a, d, False)
+    for kw in ({}, {"blocks": 3, "low_rows": 3}):
+        plan = ld.Plan(a, d, False, ld.options(**kw))
+        assert " fetch=1" in plan.describe()
+        for _ in range(3):
+            sol = plan.solve()
+            assert (sol.value, sol.gray_index) == ref
+        plan.close()
+        stat, desc = _split_of(ld, a, d, False, walk_fetch=-1, **kw)
+        assert " fetch=0" in desc and (stat.value, stat.gray_index) == ref
