@@ -747,13 +747,13 @@ def run_batch(args) -> None:
     if tail:
         solved, rest = [], []
         for idx, m, lab in sorted(tail, key=lambda x: x[2]):
-            if m.shape[0] <= args.tail_rows:
+            if args.tail_min_rows <= m.shape[0] <= args.tail_rows:
                 t0 = time.perf_counter()
                 sol = ld.solve_reduced(m, 3, False, ld.options(device=local))
                 solved.append({"index": idx, "rows": m.shape[0], "cols": m.shape[1], "labelings": lab,
                                "value": sol.value, "gray_index": sol.gray_index, "kernel_ms": sol.kernel_ms,
                                "wall_s": time.perf_counter() - t0})
-            else:
+            elif m.shape[0] > args.tail_rows:
                 rest.append({"index": idx, "rows": m.shape[0], "cols": m.shape[1], "labelings": lab})
         rate = (sum(x["labelings"] for x in solved) / max(1e-9, sum(x["kernel_ms"] for x in solved) * 1e-3)
                 if solved else None)
@@ -951,6 +951,8 @@ def main() -> None:
                     help="config 4: threads per CTA of every lane class (0 = the autotuner picks)")
     ap.add_argument("--tail-rows", type=int, default=0,
                     help="config 4: also solve the d = 3 tail matrices of at most this many rows, one by one")
+    ap.add_argument("--tail-min-rows", type=int, default=0,
+                    help="config 4: solve only the tail matrices with at least this many rows (a later part)")
     ap.add_argument("--tail-out", default="", help="config 4: write the tail's per-matrix results to this JSON file")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")

@@ -125,12 +125,16 @@ int split_bank_pad(int S, int NW, int span) {
 // matrices too wide for one thread's register vectors: over the low-row
 // counts k and the (S lanes, PW words) instances whose S x PW words hold a
 // row, the choice minimizing the table kernel's time estimate with the
-// ring's (2S - 1) instructions per labeling and the table padded to a
-// multiple of S entries.  Lanes: all 8-bit when every column passes
-// table_config's test, else all 32-bit.
-static bool split_choose(const int64_t* a, int R, int C, int d, int marginal, const ld_options& o,
-                         unsigned long long full_threads, Choice* ch) {
-  static const int kS[3] = {2, 4, 8}, kPW[3] = {8, 16, 32};
+// row padded to S x PW words, the table padded to a multiple of S entries
+// and the ring's (2S - 1) instructions per labeling, divided by an
+// occupancy factor: the kernel's accumulator chains and ring shuffles need
+// about 16 resident warps per SM to keep the integer pipe busy, and its
+// shared memory (the rows and the table in S regions) and registers decide
+// how many it gets (asked from the runtime per candidate).  Lanes: all 8-bit
+// when every column passes table_config's test, else all 32-bit.
+static bool split_choose(const int64_t* a, int R, int C, int d, int marginal, const ld_options& o, int sms,
+                         Choice* ch) {
+  static const int kS[3] = {2, 4, 8};
   const int base = d <= 2 ? 2 : d, F = R - 1;
   double best_t = 0;
   bool found = false;
@@ -158,15 +162,25 @@ static bool split_choose(const int64_t* a, int R, int C, int d, int marginal, co
     }
     for (int S : kS) {
       if (o.column_split > 0 && S != o.column_split) continue;
-      for (int PW : kPW) {
-        if (S * PW < wneed || !ld::table_split_kernel_ptr(d, PK, PW, S)) continue;
+      for (int PW = 4; PW <= 32; PW += 4) {
+        const void* fn = ld::table_split_kernel_ptr(d, PK, PW, S);
+        if (S * PW < wneed || !fn) continue;
         const int Wp = S * PW;
-        const unsigned long long Bp = (B + S - 1) / S * S;
-        if (Bp * (unsigned long long)(d * Wp) > (o.low_rows >= 0 ? 32768ull : 16384ull)) continue;
+        const int Bp = (int)((B + S - 1) / S * S);
+        const int region = ld::split_region_words(d, PW, R, Bp);
+        const size_t smem = (size_t)S * (region + 28) * sizeof(uint32_t);   // with the largest bank padding
+        int bps = 0;
+        if (smem > 227u * 1024u || ld_raise_smem_limit(fn, smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, ld::kTableThreads, smem) != cudaSuccess ||
+            bps < 1) {
+          cudaGetLastError();
+          continue;
+        }
+        const double occ = std::min(1.0, bps * (ld::kTableThreads / 32) / 16.0);
         const double words = (double)d * Wp;
         const double per_lab = (words + (2.0 * S - 1.0) / 2.0) * (double)Bp / (double)B + (2.0 * words + 40.0) / (double)B;
-        const double groups = (double)full_threads / S;
-        const double t = units * (double)B * per_lab / std::min(units, groups);
+        const double groups = (double)sms * bps * (ld::kTableThreads / S);
+        const double t = units * (double)B * per_lab / std::min(units, groups) / occ;
         if (!found || t < best_t * 0.999) {
           best_t = t;
           found = true;
@@ -228,7 +242,8 @@ ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, con
     }
     if (found) return LD_OK;
     // too wide for one thread's registers: S lanes share each high index
-    if (o.column_split >= 0 && split_choose(a, R, C, d, marginal, o, full_threads, ch)) return LD_OK;
+    if (o.column_split >= 0 && split_choose(a, R, C, d, marginal, o, (int)(full_threads / (4 * 128)), ch))
+      return LD_OK;
     if (o.column_split > 0)
       return ld_fail(LD_ERR_ARG, "no column-split instance with %d lanes takes d=%d, %d columns", o.column_split, d, C);
     if (o.kernel == LD_KERNEL_TABLE)

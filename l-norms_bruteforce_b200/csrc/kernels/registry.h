@@ -54,10 +54,11 @@ const void* batch_kernel_ptr(int D, int WB, int WA);
 const void* batch_split_kernel_ptr(int D, int WB);
 const void* batch_fold_kernel_ptr();
 // table_split_kernel<D, PK, PW, S> (split_kernel.cuh) by
-// [D][PK == 4][PW = 8, 16, 32][S = 2, 4, 8]: the column-split form of the
-// table kernel (S lanes per high index, PW words each); nullptr when not
-// instantiated.  Instances: split_d1.cu, split_d2.cu, split_d3.cu, split_dn.cu.
-using SplitKernelTab = const void* [11][2][3][3];
+// [D][PK == 4][PW / 4 - 1 (PW = 4, 8, .., 32)][S = 2, 4, 8]: the column-split
+// form of the table kernel (S lanes per high index, PW words each); nullptr
+// when not instantiated.  Instances: split_d1.cu, split_d2.cu, split_d3.cu,
+// split_dn.cu.
+using SplitKernelTab = const void* [11][2][8][3];
 void split_register_d1(SplitKernelTab& t);
 void split_register_d2(SplitKernelTab& t);
 void split_register_d3(SplitKernelTab& t);

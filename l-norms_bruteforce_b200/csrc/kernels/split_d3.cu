@@ -1,19 +1,25 @@
-// table_split_kernel<D, PK, PW, S> for D = 3: 32-bit lanes with
-// (S, PW) in (2, 32), (4, 32), (8, 16), (8, 32) (up to 256 columns), 8-bit
-// lanes with (2, 16), (4, 16), (8, 16) (up to 512 columns).
+// table_split_kernel<D, PK, PW, S> for D = 3: 32-bit lanes with PW = 16, 20,
+// .., 32 words per lane and 8-bit lanes with PW = 8, 12, 16, each for S = 2,
+// 4, 8 lanes per high index (up to 256 int32 / 512 8-bit columns; the finer
+// widths keep the padding of a row to S x PW words small).
 #include "split_inst.cuh"
 namespace ld {
 namespace {
-template <int D>
-void put_d(SplitKernelTab& t) {
-  inst::split_put<D, 1, 32, 2>(t);
-  inst::split_put<D, 1, 32, 4>(t);
-  inst::split_put<D, 1, 16, 8>(t);
-  inst::split_put<D, 1, 32, 8>(t);
-  inst::split_put<D, 4, 16, 2>(t);
-  inst::split_put<D, 4, 16, 4>(t);
-  inst::split_put<D, 4, 16, 8>(t);
+template <int D, int PK, int PW>
+void put_s(SplitKernelTab& t) {
+  inst::split_put<D, PK, PW, 2>(t);
+  inst::split_put<D, PK, PW, 4>(t);
+  inst::split_put<D, PK, PW, 8>(t);
 }
 }  // namespace
-void split_register_d3(SplitKernelTab& t) { put_d<3>(t); }
+void split_register_d3(SplitKernelTab& t) {
+  put_s<3, 1, 16>(t);
+  put_s<3, 1, 20>(t);
+  put_s<3, 1, 24>(t);
+  put_s<3, 1, 28>(t);
+  put_s<3, 1, 32>(t);
+  put_s<3, 4, 8>(t);
+  put_s<3, 4, 12>(t);
+  put_s<3, 4, 16>(t);
+}
 }  // namespace ld

@@ -1,5 +1,6 @@
 // table_split_kernel<D, PK, PW, S> for D = 4 .. 10 (register vectors D x PW):
 //   D = 4:     32-bit lanes (S, PW) in (2, 16), (4, 16), (8, 16), (8, 32)
+//   D = 4..8:  also 32-bit lanes (2, 12), (4, 12), (8, 12)
 //   D = 5..8:  32-bit lanes (2, 16), (4, 16), (8, 16)
 //   D = 9, 10: 32-bit lanes (2, 8), (4, 8), (8, 8)
 //   every D:   8-bit lanes (2, 8), (4, 8), (8, 8)
@@ -9,6 +10,9 @@ namespace {
 template <int D>
 void put_d(SplitKernelTab& t) {
   if constexpr (D <= 8) {
+    inst::split_put<D, 1, 12, 2>(t);
+    inst::split_put<D, 1, 12, 4>(t);
+    inst::split_put<D, 1, 12, 8>(t);
     inst::split_put<D, 1, 16, 2>(t);
     inst::split_put<D, 1, 16, 4>(t);
     inst::split_put<D, 1, 16, 8>(t);

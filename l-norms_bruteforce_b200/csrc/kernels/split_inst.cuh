@@ -6,7 +6,7 @@
 namespace ld {
 namespace inst {
 
-constexpr int split_pw_index(int PW) { return PW == 8 ? 0 : PW == 16 ? 1 : 2; }
+constexpr int split_pw_index(int PW) { return PW / 4 - 1; }   // PW = 4, 8, .., 32
 constexpr int split_s_index(int S) { return S == 2 ? 0 : S == 4 ? 1 : 2; }
 
 template <int D, int PK, int PW, int S>

@@ -70,7 +70,7 @@ const void* table_split_kernel_ptr(int D, int PK, int PW, int S) {
     return true;
   }();
   (void)init;
-  const int pi = PW == 8 ? 0 : PW == 16 ? 1 : PW == 32 ? 2 : -1;
+  const int pi = (PW >= 4 && PW <= 32 && PW % 4 == 0) ? PW / 4 - 1 : -1;
   const int si = S == 2 ? 0 : S == 4 ? 1 : S == 8 ? 2 : -1;
   if (D < 1 || D > 10 || (PK != 1 && PK != 4) || pi < 0 || si < 0) return nullptr;
   return tab[D][PK == 4 ? 1 : 0][pi][si];
