@@ -498,7 +498,9 @@ def run_ours(args) -> None:
     if (info["rows"], info["cols"], int(info["labelings"])) != (cfg["rows"], cfg["cols"], cfg["labelings_per_step"]):
         raise RuntimeError(f"preprocessing left {info['rows']}x{info['cols']}, the workload says "
                            f"{cfg['rows']}x{cfg['cols']}")
-    opts = ld.options(device=local, shard_index=rank, shard_count=world)
+    knobs = dict(column_split=args.column_split, walk_fetch=args.walk_fetch, pack16=args.pack16,
+                 paired_walks=args.paired_walks)
+    opts = ld.options(device=local, shard_index=rank, shard_count=world, **knobs)
     plan = ld.Plan(red, d, marg, opts)
     lo, hi = plan.range
     total_labelings = info["labelings"]
@@ -557,7 +559,7 @@ def run_ours(args) -> None:
             dist.barrier()
         t0 = time.perf_counter()
         p = ld.Problem.from_matrix(inst.matrix, inst.d, inst.stat, inst.marginal)
-        res = p.solve(ld.options(device=local, shard_index=rank, shard_count=world))
+        res = p.solve(ld.options(device=local, shard_index=rank, shard_count=world, **knobs))
         if world > 1:
             res.value, res.gray_index = D.combine(int(res.value), int(res.gray_index),
                                                   device=torch.device("cuda", local))
@@ -937,6 +939,11 @@ def main() -> None:
                     help="plain runs: instead of a configuration, a seeded matrix with this many columns "
                          "(the column-split table kernel's workload)")
     ap.add_argument("--wide-d", type=int, default=1, help="order d of the --wide matrix")
+    for knob, what in (("column-split", "lanes per high index (2, 4, 8; -1 never; 0 auto)"),
+                       ("walk-fetch", "0 warps fetch walks from a counter, -1 fixed split"),
+                       ("pack16", "0 packed 16-bit maxima when values allow, -1 never"),
+                       ("paired-walks", "0 two high indices per thread when possible, -1 never")):
+        ap.add_argument(f"--{knob}", type=int, default=0, help=f"plain runs, table kernel knob: {what}")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--method", default="plain", choices=["plain", "pruned", "learned"],
                     help="plain enumeration (the headline), or the exact pruned search with an "

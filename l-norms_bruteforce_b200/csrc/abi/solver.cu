@@ -179,8 +179,10 @@ static bool split_choose(const int64_t* a, int R, int C, int d, int marginal, co
         const double occ = std::min(1.0, bps * (ld::kTableThreads / 32) / 16.0);
         const double words = (double)d * Wp;
         const double per_lab = (words + (2.0 * S - 1.0) / 2.0) * (double)Bp / (double)B + (2.0 * words + 40.0) / (double)B;
+        // an SM's throughput scales with the occupancy factor; groups
+        // without a high index to walk add nothing
         const double groups = (double)sms * bps * (ld::kTableThreads / S);
-        const double t = units * (double)B * per_lab / std::min(units, groups) / occ;
+        const double t = units * (double)B * per_lab / ((double)sms * occ) / std::min(1.0, units / groups);
         if (!found || t < best_t * 0.999) {
           best_t = t;
           found = true;

@@ -77,6 +77,54 @@ __device__ __forceinline__ int split_tile(const uint32_t* H, const uint32_t* sT,
   return (int)acc[0];
 }
 
+// Two tiles at once (entries j0 .. j0 + 2S - 1): 2S independent partial
+// sums, then the two rings interleaved, so that each shuffle's latency is
+// hidden behind the other ring's step.  v0 / v1: entry j0 + g / j0 + S + g.
+template <int D, int SB, int SA, int S>
+__device__ __forceinline__ void split_tile2(const uint32_t* H, const uint32_t* sT, int j0, int g, unsigned gmask,
+                                            int src, int& v0, int& v1) {
+  using Sh = Shape<D, SB, SA>;
+  uint32_t acc[S], acd[S];
+#pragma unroll
+  for (int r = 0; r < S; ++r) {
+    const int e = (g + r) & (S - 1);
+    const uint4* t0 = reinterpret_cast<const uint4*>(sT + (j0 + e) * Sh::NW);
+    const uint4* t1 = reinterpret_cast<const uint4*>(sT + (j0 + S + e) * Sh::NW);
+    uint32_t a0 = 0u, a1 = 0u, b0 = 0u, b1 = 0u;
+#pragma unroll
+    for (int q = 0; q < Sh::NW / 4; ++q) {
+      sad4<D, SB, SA>(H, t0[q], q, a0, a1);
+      sad4<D, SB, SA>(H, t1[q], q, b0, b1);
+    }
+    acc[r] = a0 + a1;
+    acd[r] = b0 + b1;
+  }
+#pragma unroll
+  for (int t = 1; t < S; ++t) {
+    const uint32_t x = __shfl_sync(gmask, acc[S - t], src, S);
+    const uint32_t y = __shfl_sync(gmask, acd[S - t], src, S);
+    acc[S - 1 - t] += x;
+    acd[S - 1 - t] += y;
+  }
+  v0 = (int)acc[0];
+  v1 = (int)acd[0];
+}
+
+// max over the Bp table entries: pairs of tiles, then a last single tile
+template <int D, int SB, int SA, int S>
+__device__ __forceinline__ int split_scan(const uint32_t* H, const uint32_t* sT, int Bp, int g, unsigned gmask,
+                                          int src) {
+  int m = INT_MIN;
+  int j0 = 0;
+  for (; j0 + 2 * S <= Bp; j0 += 2 * S) {
+    int v0, v1;
+    split_tile2<D, SB, SA, S>(H, sT, j0, g, gmask, src, v0, v1);
+    m = max(m, max(v0, v1));
+  }
+  if (j0 < Bp) m = max(m, split_tile<D, SB, SA, S>(H, sT, j0, g, gmask, src));
+  return m;
+}
+
 template <int D, int PK, int PW, int S>
 __global__ void __launch_bounds__(kTableThreads) table_split_kernel(const SplitArgs sa) {
   static_assert(PK == 1 || PK == 4, "32-bit lanes or four 8-bit lanes per word");
@@ -140,8 +188,7 @@ __global__ void __launch_bounds__(kTableThreads) table_split_kernel(const SplitA
         high_step<D>(wk, h0 + u, u, i, a, b);
         move_row<D, SB, SA>(H, sA + (k + i) * PW, a, b);
       }
-      int m = INT_MIN;
-      for (int j0 = 0; j0 < Bp; j0 += S) m = max(m, split_tile<D, SB, SA, S>(H, sT, j0, g, gmask, src));
+      const int m = split_scan<D, SB, SA, S>(H, sT, Bp, g, gmask, src);
       if (m > best) { best = m; best_h = h0 + u; }
     }
   }
