@@ -134,3 +134,22 @@ def test_batch_column_split(ld, split):
     assert ("column split" in desc) == (split == 1), desc
     for p, (a, d, m) in enumerate(zip(mats, ds, ms)):
         assert (int(v[p]), int(g[p])) == O.enumerate_max(a, d, bool(m)), (p, a.shape, d, m, desc)
+
+
+def test_config4_tail_matches_oracle(ld, workloads):
+    """The d = 3 tail of the 4096-matrix workload (more than 3^20 labelings
+    each, solved one by one outside the batch replay): its smallest
+    matrices, 22 rows (3^21 labelings), against values the oracle computed
+    on the CPU (tests/golden/make_tail_golden.py; about a minute each
+    there, some 20-30 ms here)."""
+    import json
+    from pathlib import Path
+    gold = json.loads((Path(__file__).parent / "golden" / "config4_tail.json").read_text())
+    insts = workloads.config4()
+    assert len(gold) >= 3
+    for g in gold:
+        p = ld.Problem.from_matrix(insts[g["index"]].matrix, insts[g["index"]].d)
+        red = p.reduced
+        assert red.shape == (g["rows"], g["cols"]) and p.info["d"] == 3
+        sol = ld.solve_reduced(red, 3)
+        assert (sol.value, sol.gray_index) == (g["value"], g["gray_index"]), g["index"]
