@@ -1,7 +1,8 @@
 // table_split_kernel<D, PK, PW, S> for D = 1: 32-bit lanes with PW = 16, 20,
 // .., 32 words per lane and 8-bit lanes with PW = 8, 12, 16, each for S = 2,
 // 4, 8 lanes per high index (up to 256 int32 / 512 8-bit columns; the finer
-// widths keep the padding of a row to S x PW words small).
+// widths keep the padding of a row to S x PW words small).  Two high
+// indices per group (K = 2).
 #include "split_inst.cuh"
 namespace ld {
 namespace {

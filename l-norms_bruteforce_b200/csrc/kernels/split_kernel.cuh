@@ -125,10 +125,52 @@ __device__ __forceinline__ int split_scan(const uint32_t* H, const uint32_t* sT,
   return m;
 }
 
-template <int D, int PK, int PW, int S>
+// Two high indices per group (K = 2): a tile's slice of each entry is read
+// from shared memory once and compared with both register vectors H and G.
+// Each lane needs its own 16 bytes per four absolute-difference-accumulates
+// (the S lanes of a group read different slices, so the read is not a
+// broadcast as in the table kernel), which at one high index per lane asks
+// twice what shared memory delivers (128 bytes per clock per SM) at the
+// integer pipe's rate; two halve it.  mh / mg: the maxima for H and G.
+template <int D, int SB, int SA, int S>
+__device__ __forceinline__ void split_scan2(const uint32_t* H, const uint32_t* G, const uint32_t* sT, int Bp, int g,
+                                            unsigned gmask, int src, int& mh, int& mg) {
+  using Sh = Shape<D, SB, SA>;
+  int m0 = INT_MIN, m1 = INT_MIN;
+  for (int j0 = 0; j0 < Bp; j0 += S) {
+    uint32_t acc[S], acg[S];
+#pragma unroll
+    for (int r = 0; r < S; ++r) {
+      const uint4* t = reinterpret_cast<const uint4*>(sT + (j0 + ((g + r) & (S - 1))) * Sh::NW);
+      uint32_t a0 = 0u, a1 = 0u, b0 = 0u, b1 = 0u;
+#pragma unroll
+      for (int q = 0; q < Sh::NW / 4; ++q) {
+        const uint4 x = t[q];
+        sad4<D, SB, SA>(H, x, q, a0, a1);
+        sad4<D, SB, SA>(G, x, q, b0, b1);
+      }
+      acc[r] = a0 + a1;
+      acg[r] = b0 + b1;
+    }
+#pragma unroll
+    for (int t = 1; t < S; ++t) {
+      const uint32_t x = __shfl_sync(gmask, acc[S - t], src, S);
+      const uint32_t y = __shfl_sync(gmask, acg[S - t], src, S);
+      acc[S - 1 - t] += x;
+      acg[S - 1 - t] += y;
+    }
+    m0 = max(m0, (int)acc[0]);
+    m1 = max(m1, (int)acg[0]);
+  }
+  mh = m0;
+  mg = m1;
+}
+
+template <int D, int PK, int PW, int S, int K = 1>
 __global__ void __launch_bounds__(kTableThreads) table_split_kernel(const SplitArgs sa) {
   static_assert(PK == 1 || PK == 4, "32-bit lanes or four 8-bit lanes per word");
   static_assert(PW % 4 == 0 && (S == 2 || S == 4 || S == 8), "slices of whole 16-byte words, 2-8 lanes");
+  static_assert(K == 1 || (K == 2 && D <= 2), "two high indices per group: d <= 2 (one register vector each)");
   constexpr int SB = PK == 1 ? PW : 0, SA = PK == 4 ? PW : 0;
   using Sh = Shape<D, SB, SA>;   // one slice: WV = WT = PW
   constexpr int NW = Sh::NW;     // words of a slice entry (D * PW)
@@ -175,6 +217,30 @@ __global__ void __launch_bounds__(kTableThreads) table_split_kernel(const SplitA
   // lanes of a group take the same walks (same control flow for the shuffles)
   const bool by_rank = D >= 3 && args.sym_digits > 0;
   const unsigned long long it_end = by_rank ? args.rank_end : args.walk_end;
+  if constexpr (K == 2) {
+    // walks it and it + G in lockstep: the same row moves at each step (the
+    // step depends on the offset only); a lone last walk runs twice
+    uint32_t G2[Sh::NR * PW];
+    for (unsigned long long it = args.walk_begin + gid; it < it_end; it += 2 * G) {
+      const unsigned long long wk = it, wg = it + G < it_end ? it + G : it;
+      const unsigned long long h0 = wk * WL, g0 = wg * WL;
+      seed_high<D, SB, SA>(H, sA, sH0, k, nh, h0);
+      seed_high<D, SB, SA>(G2, sA, sH0, k, nh, g0);
+      for (unsigned long long u = 0; u < WL; ++u) {
+        if (u) {
+          int i, a, b, i2, a2, b2;
+          high_step<D>(wk, h0 + u, u, i, a, b);
+          high_step<D>(wg, g0 + u, u, i2, a2, b2);
+          move_row<D, SB, SA>(H, sA + (k + i) * PW, a, b);
+          move_row<D, SB, SA>(G2, sA + (k + i2) * PW, a2, b2);
+        }
+        int mh, mg;
+        split_scan2<D, SB, SA, S>(H, G2, sT, Bp, g, gmask, src, mh, mg);
+        if (mh > best || (mh == best && h0 + u < best_h)) { best = mh; best_h = h0 + u; }
+        if (mg > best || (mg == best && g0 + u < best_h)) { best = mg; best_h = g0 + u; }
+      }
+    }
+  } else {
   for (unsigned long long it = (by_rank ? args.rank_begin : args.walk_begin) + gid; it < it_end; it += G) {
     unsigned long long wk = it;
     if constexpr (D >= 3) {
@@ -191,6 +257,7 @@ __global__ void __launch_bounds__(kTableThreads) table_split_kernel(const SplitA
       const int m = split_scan<D, SB, SA, S>(H, sT, Bp, g, gmask, src);
       if (m > best) { best = m; best_h = h0 + u; }
     }
+  }
   }
 
   // the group's maximum and the smallest high index attaining it
