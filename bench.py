@@ -954,7 +954,7 @@ def main() -> None:
     ap.add_argument("--batch-split", type=int, default=0, choices=(-1, 0, 1),
                     help="config 4: column-split instances of the wide int32 classes "
                          "(0 = the autotuner picks, 1 = always, -1 = never)")
-    ap.add_argument("--batch-tpb", type=int, default=0, choices=(0, 64, 128, 256),
+    ap.add_argument("--batch-tpb", type=int, default=0, choices=(0, 64, 128),
                     help="config 4: threads per CTA of every lane class (0 = the autotuner picks)")
     ap.add_argument("--tail-rows", type=int, default=0,
                     help="config 4: also solve the d = 3 tail matrices of at most this many rows, one by one")

@@ -32,8 +32,9 @@ using namespace ldsolve;
 
 namespace {
 
-// threads per CTA the autotuner tries
-constexpr int kTpbChoices[3] = {64, 128, 256};
+// threads per CTA the autotuner tries (the kernels' launch bound is 128)
+constexpr int kTpbN = 2;
+constexpr int kTpbChoices[kTpbN] = {64, 128};
 
 struct BatchClass {
   int D = 0, WB = 0, WA = 0;
@@ -48,12 +49,12 @@ struct BatchClass {
   int bps_split = 0;
   bool split = false;             // the autotuner chose the column-split instance
   int tpb = ld::kBatchThreads;    // threads per CTA (chunks hold tpb * wpt walks)
-  int occ[2][3] = {{0, 0, 0}, {0, 0, 0}};  // resident CTAs per SM: [split][kTpbChoices index]
+  int occ[2][kTpbN] = {{0, 0}, {0, 0}};  // resident CTAs per SM: [split][kTpbChoices index]
   float tuned[2] = {0.f, 0.f};    // autotuner: best ms per 1e9 labelings, plain / split instance
   const void* fn() const { return split ? kfn_split : kfn; }
   size_t shm() const { return split ? smem_split : smem; }
   int blocks_per_sm() const {
-    for (int t = 0; t < 3; ++t)
+    for (int t = 0; t < kTpbN; ++t)
       if (kTpbChoices[t] == tpb) return occ[split ? 1 : 0][t];
     return 0;
   }
@@ -282,7 +283,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     std::stable_sort(c.probs.begin(), c.probs.end(),
                      [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
     bool ok = ld_raise_smem_limit(c.kfn, c.smem) == cudaSuccess;
-    for (int t = 0; t < 3 && ok; ++t)
+    for (int t = 0; t < kTpbN && ok; ++t)
       ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ[0][t], c.kfn, kTpbChoices[t], c.smem) == cudaSuccess;
     c.bps = c.occ[0][1];
     if (!ok || c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -292,7 +293,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     }
     if (c.kfn_split) {
       bool sok = ld_raise_smem_limit(c.kfn_split, c.smem_split) == cudaSuccess;
-      for (int t = 0; t < 3 && sok; ++t)
+      for (int t = 0; t < kTpbN && sok; ++t)
         sok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ[1][t], c.kfn_split, kTpbChoices[t],
                                                             c.smem_split) == cudaSuccess;
       c.bps_split = c.occ[1][1];
@@ -436,7 +437,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     return LD_OK;
   };
   for (auto& c : b->classes) {
-    if (o.threads_per_block == 64 || o.threads_per_block == 128 || o.threads_per_block == 256)
+    if (o.threads_per_block == 64 || o.threads_per_block == 128)
       c.tpb = o.threads_per_block;
     double mean = 0;
     for (int p : c.probs) mean += (double)walks[p];

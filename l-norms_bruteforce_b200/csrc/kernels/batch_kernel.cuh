@@ -41,10 +41,13 @@ struct BatchArgs {
   Slot* chunk_results;      // one per chunk
 };
 
-// Threads per CTA: the autotuner picks 64, 128 or 256 per lane class (the
-// kernels read blockDim); 128 is the default.
+// Threads per CTA: the autotuner picks 64 or 128 per lane class (the
+// kernels read blockDim); 128 is the default and the launch bound.  A bound
+// of 256 (to offer 256-thread CTAs) changed the register allocation of the
+// int32 classes (48 words: 127 -> 164 registers, a resident CTA less per
+// SM) and cost 2.5 % of the batch replay, more than the larger CTAs gained.
 constexpr int kBatchThreads = 128;
-constexpr int kBatchMaxThreads = 256;
+constexpr int kBatchMaxThreads = 128;
 
 // block-wide (max value, smallest index); the result is valid in thread 0
 __device__ __forceinline__ void block_best(long long& v, unsigned long long& n) {
