@@ -499,7 +499,7 @@ def run_ours(args) -> None:
         raise RuntimeError(f"preprocessing left {info['rows']}x{info['cols']}, the workload says "
                            f"{cfg['rows']}x{cfg['cols']}")
     knobs = dict(column_split=args.column_split, walk_fetch=args.walk_fetch, pack16=args.pack16,
-                 paired_walks=args.paired_walks)
+                 paired_walks=args.paired_walks, tile=args.tile)
     opts = ld.options(device=local, shard_index=rank, shard_count=world, **knobs)
     plan = ld.Plan(red, d, marg, opts)
     lo, hi = plan.range
@@ -942,7 +942,8 @@ def main() -> None:
     for knob, what in (("column-split", "lanes per high index (2, 4, 8; -1 never; 0 auto)"),
                        ("walk-fetch", "0 warps fetch walks from a counter, -1 fixed split"),
                        ("pack16", "0 packed 16-bit maxima when values allow, -1 never"),
-                       ("paired-walks", "0 two high indices per thread when possible, -1 never")):
+                       ("paired-walks", "0 two high indices per thread when possible, -1 never"),
+                       ("tile", "high-row digits per walk (0 auto)")):
         ap.add_argument(f"--{knob}", type=int, default=0, help=f"plain runs, table kernel knob: {what}")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--method", default="plain", choices=["plain", "pruned", "learned"],
