@@ -207,7 +207,9 @@ static bool split_choose(const int64_t* a, int R, int C, int d, int marginal, co
 // an estimate of the solve time: labelings x (words per labeling + the
 // amortized cost of a high-row step) / threads that have work.
 ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, const Bounds& b,
-                        const ld_options& o, unsigned long long full_threads, Choice* ch) {
+                        const ld_options& o, int sms, Choice* ch) {
+  // threads of a full grid for the time estimate: 4 blocks of 128 per SM
+  const unsigned long long full_threads = (unsigned long long)sms * 4 * 128;
   if (b.overflow) return ld_fail(LD_ERR_LIMIT, "matrix entries too large: column sums exceed 2^61");
   const long long maxabs = std::max(b.colbound, marginal ? 2 * b.K : 0LL);
   const long long vmax = b.total + (marginal ? b.K : 0LL);
@@ -244,8 +246,7 @@ ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, con
     }
     if (found) return LD_OK;
     // too wide for one thread's registers: S lanes share each high index
-    if (o.column_split >= 0 && split_choose(a, R, C, d, marginal, o, (int)(full_threads / (4 * 128)), ch))
-      return LD_OK;
+    if (o.column_split >= 0 && split_choose(a, R, C, d, marginal, o, sms, ch)) return LD_OK;
     if (o.column_split > 0)
       return ld_fail(LD_ERR_ARG, "no column-split instance with %d lanes takes d=%d, %d columns", o.column_split, d, C);
     if (o.kernel == LD_KERNEL_TABLE)
@@ -416,7 +417,7 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
   p->R = R; p->C = C; p->d = d; p->marginal = marginal;
   p->total = total;
   p->bounds = compute_bounds(a, R, C, marginal);
-  st = choose_kernel(a, R, C, d, marginal, p->bounds, o, (unsigned long long)di.sms * 4 * 128, &p->ch);
+  st = choose_kernel(a, R, C, d, marginal, p->bounds, o, di.sms, &p->ch);
   if (st != LD_OK) { delete p; return st; }
 
   const int base = d <= 2 ? 2 : d;
@@ -453,7 +454,8 @@ ld_status ldsolve::plan_build(const int64_t* a, int R, int C, int d, int margina
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, p->kfn, p->tpb, p->smem) != cudaSuccess || bps < 1) {
       delete p; return ld_fail(LD_ERR_CUDA, "table kernel does not fit an SM (smem %zu)", p->smem);
     }
-    p->pack16 = (o.pack16 >= 0 && p->bounds.total + 2 * (marginal ? p->bounds.K : 0) < 65536) ? 1 : 0;
+    // packed maxima: the table kernel's scans (the column split keeps one maximum per word)
+    p->pack16 = (p->ch.S == 0 && o.pack16 >= 0 && p->bounds.total + 2 * (marginal ? p->bounds.K : 0) < 65536) ? 1 : 0;
     // parallel units of a full grid: threads, or groups of S lanes
     const unsigned long long full = (unsigned long long)di.sms * bps * (p->tpb / S);
     const int nh = F - k;

@@ -57,7 +57,7 @@ inline unsigned long long ipow(unsigned long long b, int e) {
 bool table_config(const int64_t* a, int R, int C, int d, int marginal, int k, int force_bits, Choice* ch);
 int split_bank_pad(int S, int NW, int span);
 ld_status choose_kernel(const int64_t* a, int R, int C, int d, int marginal, const Bounds& b,
-                        const ld_options& o, unsigned long long full_threads, Choice* ch);
+                        const ld_options& o, int sms, Choice* ch);
 void pack_row(const int64_t* row, const Choice& ch, uint32_t* out);
 
 struct DeviceInfo {
