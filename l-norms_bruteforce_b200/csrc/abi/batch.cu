@@ -49,6 +49,7 @@ struct BatchClass {
   int bps_split = 0;
   bool split = false;             // the autotuner chose the column-split instance
   int tpb = ld::kBatchThreads;    // threads per CTA (chunks hold tpb * wpt walks)
+  int kshift = 0;                 // low rows below the largest table that fits, for every matrix
   int occ[2][kTpbN] = {{0, 0}, {0, 0}};  // resident CTAs per SM: [split][kTpbChoices index]
   float tuned[2] = {0.f, 0.f};    // autotuner: best ms per 1e9 labelings, plain / split instance
   const void* fn() const { return split ? kfn_split : kfn; }
@@ -64,9 +65,9 @@ struct BatchClass {
 };
 
 // autotuner cache: (D, WB, WA, log2 of the mean walks per problem, batch_split option)
-//   -> (wpt, grid fraction, split, threads per CTA)
+//   -> (wpt, grid fraction, split, threads per CTA, low-row shift)
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool, int>> g_tune;
+std::map<std::tuple<int, int, int, int, int>, std::tuple<int, double, bool, int, int>> g_tune;
 
 }  // namespace
 
@@ -152,8 +153,68 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   b->range_first.assign(count, 0);
   b->range_end.assign(count, 0);
   std::vector<unsigned long long> walks(count, 0);
+  std::vector<unsigned long long> max_walks(count, 0);   // over the low-row counts the tuner tries
   std::vector<std::vector<char>> images(count);
+  std::vector<Choice> pch(count);                        // lane layout per class matrix
+  std::vector<int> kmax(count, -1);                      // the largest low-row count that fits
   std::map<std::tuple<int, int, int>, int> class_of;
+  b->hprob.resize(count);
+  // walks of matrix p at low-row count k: whole high indices, at most about
+  // 2^16 walks (enough chunks to spread one large matrix); fw = walked digits
+  auto walk_geometry = [&](int p, int k, int* fw_out) -> unsigned long long {
+    const int d = ds[p], base = d <= 2 ? 2 : d, nh = rows[p] - 1 - k;
+    int fw = 0;
+    while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 16.0) ++fw;
+    if (fw_out) *fw_out = fw;
+    return ipow(base, nh - fw);
+  };
+  // Geometry, image and problem-table entry of class matrix p at low-row
+  // count k (the device pointers of its entry are kept).  The rows' image
+  // does not depend on k; for LM the initial H and the table bias do (the
+  // low rows' and the other rows' share of the column-0 shift).
+  auto geometry = [&](int p, int k) {
+    const int R = rows[p], C = cols[p], d = ds[p], marg = margs ? margs[p] : 0;
+    const int64_t* a = mats[p];
+    const Choice& ch = pch[p];
+    const int base = d <= 2 ? 2 : d, nh = R - 1 - k;
+    int fw = 0;
+    walks[p] = walk_geometry(p, k, &fw);
+    const int B = (int)ipow(base, k), WT = ch.WT;
+    // image: tot | h0 | tb | rows (each vector padded to 256 bytes)
+    std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
+    long long kl = 0, kh = 0;
+    for (int i = 0; i < R; ++i)
+      for (int l = 0; l < C; ++l) tot[l] += a[(size_t)i * C + l];
+    if (d == 1) {
+      for (int l = 0; l < C; ++l) h0[l] = a[(size_t)(R - 1) * C + l];
+      if (marg) {
+        for (int i = 0; i < R; ++i) { const int64_t v = a[(size_t)i * C]; (i < k ? kl : kh) += v < 0 ? -v : v; }
+        h0[0] += kh; tb[0] = -kl;
+      }
+    }
+    std::vector<char>& img = images[p];
+    img.assign(768 + align256((size_t)R * WT * 4), 0);
+    pack_row(tot.data(), ch, (uint32_t*)(img.data() + 0));
+    pack_row(h0.data(), ch, (uint32_t*)(img.data() + 256));
+    pack_row(tb.data(), ch, (uint32_t*)(img.data() + 512));
+    for (int i = 0; i < R; ++i) pack_row(a + (size_t)i * C, ch, (uint32_t*)(img.data() + 768) + (size_t)i * WT);
+    ld::BatchProblem bp = b->hprob[p];   // keeps the device pointers
+    bp.R = R; bp.k = k; bp.B = B; bp.fw = fw;
+    bp.walk_len = ipow(base, fw);
+    bp.sym_digits = 0;
+    bp.sym_pw = 1;
+    uint64_t run = walks[p];
+    if (d == 3 && !o.enumerate_all && nh - fw > 0 &&
+        ld_symmetry_walks(d, nh - fw, 0, walks[p], &run) == LD_OK) {
+      bp.sym_digits = nh - fw;
+      bp.sym_pw = ipow(base, nh - fw - 1);
+    } else {
+      run = walks[p];
+    }
+    b->evaluated[p] = (unsigned long long)run * bp.walk_len * (unsigned long long)B;
+    bp.value_offset = kh + kl;
+    b->hprob[p] = bp;
+  };
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
@@ -231,66 +292,29 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
       ci = it->second;
     }
     b->cls[p] = ci;
-    BatchClass& bc = b->classes[ci];
-    bc.probs.push_back(p);
-    const int nh = F - k;
-    // walks per matrix: at most 2^16 (enough chunks to spread one large matrix)
-    int fw = 0;
-    while (fw < nh && (double)(nh - fw) * std::log2((double)base) > 16.0) ++fw;
-    walks[p] = ipow(base, nh - fw);
-    const int B = (int)ipow(base, k), WT = ch.WT;
-    bc.smem = std::max(bc.smem, (size_t)ld::table_smem_words(d, WT, R, B) * 4);
-    if (bc.kfn_split)
-      bc.smem_split = std::max(bc.smem_split, (size_t)ld::batch_split_smem_words(d, ch.WB, R, B) * 4);
-    // image: tot | h0 | tb | rows (each vector padded to 256 bytes)
-    std::vector<int64_t> tot(C, 0), h0(C, 0), tb(C, 0);
-    long long kl = 0, kh = 0;
-    for (int i = 0; i < R; ++i)
-      for (int l = 0; l < C; ++l) tot[l] += a[(size_t)i * C + l];
-    if (d == 1) {
-      for (int l = 0; l < C; ++l) h0[l] = a[(size_t)(R - 1) * C + l];
-      if (marg) {
-        for (int i = 0; i < R; ++i) { const int64_t v = a[(size_t)i * C]; (i < k ? kl : kh) += v < 0 ? -v : v; }
-        h0[0] += kh; tb[0] = -kl;
-      }
-    }
-    std::vector<char>& img = images[p];
-    img.assign(768 + align256((size_t)R * WT * 4), 0);
-    pack_row(tot.data(), ch, (uint32_t*)(img.data() + 0));
-    pack_row(h0.data(), ch, (uint32_t*)(img.data() + 256));
-    pack_row(tb.data(), ch, (uint32_t*)(img.data() + 512));
-    for (int i = 0; i < R; ++i) pack_row(a + (size_t)i * C, ch, (uint32_t*)(img.data() + 768) + (size_t)i * WT);
-    ld::BatchProblem bp{};
-    bp.R = R; bp.k = k; bp.B = B; bp.fw = fw;
-    bp.walk_len = ipow(base, fw);
-    bp.sym_pw = 1;
-    uint64_t run = walks[p];
-    if (d == 3 && !o.enumerate_all && nh - fw > 0 &&
-        ld_symmetry_walks(d, nh - fw, 0, walks[p], &run) == LD_OK) {
-      bp.sym_digits = nh - fw;
-      bp.sym_pw = ipow(base, nh - fw - 1);
-    } else {
-      run = walks[p];
-    }
-    b->evaluated[p] = (unsigned long long)run * bp.walk_len * (unsigned long long)B;
-    bp.value_offset = kh + kl;
-    b->hprob.resize(count);
-    b->hprob[p] = bp;
+    b->classes[ci].probs.push_back(p);
+    pch[p] = ch;
+    kmax[p] = k;
+    geometry(p, k);
+    // the tuner may lower k by up to 2 for int32 classes: more walks
+    max_walks[p] = ch.WA == 0 ? walk_geometry(p, std::max(0, k - 2), nullptr) : walks[p];
   }
-  b->hprob.resize(count);
-  // classes: largest matrices first, occupancy, streams
-  for (auto& c : b->classes) {
-    std::stable_sort(c.probs.begin(), c.probs.end(),
-                     [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
+  // a class's shared memory (its largest matrix table) and occupancy, for
+  // the current geometry of its matrices
+  auto class_fit = [&](BatchClass& c) -> bool {
+    c.smem = 0;
+    c.smem_split = 0;
+    for (int p : c.probs) {
+      const ld::BatchProblem& bp = b->hprob[p];
+      c.smem = std::max(c.smem, (size_t)ld::table_smem_words(c.D, pch[p].WT, bp.R, bp.B) * 4);
+      if (c.kfn_split)
+        c.smem_split = std::max(c.smem_split, (size_t)ld::batch_split_smem_words(c.D, c.WB, bp.R, bp.B) * 4);
+    }
     bool ok = ld_raise_smem_limit(c.kfn, c.smem) == cudaSuccess;
     for (int t = 0; t < kTpbN && ok; ++t)
       ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ[0][t], c.kfn, kTpbChoices[t], c.smem) == cudaSuccess;
     c.bps = c.occ[0][1];
-    if (!ok || c.bps < 1 || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
-      batch_free(b);
-      return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d WA=%d does not fit an SM", c.D, c.WB, c.WA);
-    }
+    if (!ok || c.bps < 1) return false;
     if (c.kfn_split) {
       bool sok = ld_raise_smem_limit(c.kfn_split, c.smem_split) == cudaSuccess;
       for (int t = 0; t < kTpbN && sok; ++t)
@@ -301,6 +325,17 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
         cudaGetLastError();
         c.kfn_split = nullptr;
       }
+    }
+    return true;
+  };
+  // classes: largest matrices first, occupancy, streams
+  for (auto& c : b->classes) {
+    std::stable_sort(c.probs.begin(), c.probs.end(),
+                     [&](int x, int y) { return b->labelings[x] > b->labelings[y]; });
+    if (!class_fit(c) || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
+      batch_free(b);
+      return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d WA=%d does not fit an SM", c.D, c.WB, c.WA);
     }
   }
   // device memory: images, problem table, chunks (sized for the largest wpt
@@ -314,7 +349,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
   for (auto& c : b->classes) {
     BatchClass tc = c;
     tc.tpb = kTpbChoices[0];
-    max_chunks += batch_chunks(b, tc, 1, walks, nullptr);
+    max_chunks += batch_chunks(b, tc, 1, max_walks, nullptr);
   }
   b->off_prob = bytes;   bytes += align256(sizeof(ld::BatchProblem) * count);
   b->off_chunks = bytes; bytes += align256(sizeof(ld::BatchChunk) * std::max(1, max_chunks));
@@ -436,6 +471,20 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     *per_out = (float)(ms[reps / 2] / std::max(1.0, lab));
     return LD_OK;
   };
+  // the class's matrices at their largest low-row count lowered by `shift`
+  // (int32 classes only: there the lane layout does not depend on k),
+  // uploaded: problem-table entries and the image vectors that depend on k
+  auto apply_shift = [&](BatchClass& c, int shift) -> ld_status {
+    for (int p : c.probs) {
+      geometry(p, std::max(0, kmax[p] - shift));
+      LD_CUDA(cudaMemcpy(b->dmem + img_off[p], images[p].data(), 768, cudaMemcpyHostToDevice));
+      LD_CUDA(cudaMemcpy(b->dmem + b->off_prob + sizeof(ld::BatchProblem) * p, &b->hprob[p],
+                         sizeof(ld::BatchProblem), cudaMemcpyHostToDevice));
+    }
+    c.kshift = shift;
+    if (!class_fit(c)) return ld_fail(LD_ERR_CUDA, "batch class D=%d WB=%d does not fit an SM", c.D, c.WB);
+    return LD_OK;
+  };
   for (auto& c : b->classes) {
     if (o.threads_per_block == 64 || o.threads_per_block == 128)
       c.tpb = o.threads_per_block;
@@ -448,7 +497,12 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune.find(key);
       if (it != g_tune.end()) {
-        std::tie(c.wpt, c.grid_frac, c.split, c.tpb) = it->second;
+        int shift = 0;
+        std::tie(c.wpt, c.grid_frac, c.split, c.tpb, shift) = it->second;
+        if (shift > 0) {
+          st = apply_shift(c, shift);
+          if (st != LD_OK) { batch_free(b); return st; }
+        }
         if (!c.kfn_split) c.split = false;
         if (o.batch_split > 0 && c.kfn_split) c.split = true;
         if (c.blocks_per_sm() < 1) { c.tpb = ld::kBatchThreads; }
@@ -457,31 +511,49 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     }
     if (o.batch_split > 0 && c.kfn_split) c.split = true;
     if (!autotune) continue;
-    std::vector<Cand> cands;
-    for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
-      for (int tpb : kTpbChoices) {
-        if (o.threads_per_block > 0 && tpb != o.threads_per_block) continue;   // forced block shape
-        for (int wpt : {1, 2, 4, 8})
-          for (double frac : {0.5, 1.0}) cands.push_back(Cand{variant, tpb, wpt, frac, 1e30f});
+    // low-row counts: the largest that fits (shift 0) and, for int32
+    // classes, one or two rows fewer (smaller tables, more walks)
+    int max_shift = 0;
+    if (c.WA == 0)
+      for (int p : c.probs) max_shift = std::max(max_shift, std::min(2, kmax[p]));
+    Cand best{0, c.tpb, c.wpt, c.grid_frac, 1e30f};
+    int best_shift = 0;
+    for (int shift = 0; shift <= max_shift; ++shift) {
+      if (shift != c.kshift) {
+        st = apply_shift(c, shift);
+        if (st != LD_OK) { batch_free(b); return st; }
       }
-    for (auto& cd : cands) {
-      st = time_cand(c, cd, 1, &cd.per);
+      std::vector<Cand> cands;
+      for (int variant = o.batch_split > 0 && c.kfn_split ? 1 : 0; variant < (c.kfn_split ? 2 : 1); ++variant)
+        for (int tpb : kTpbChoices) {
+          if (o.threads_per_block > 0 && tpb != o.threads_per_block) continue;   // forced block shape
+          for (int wpt : {1, 2, 4, 8})
+            for (double frac : {0.5, 1.0}) cands.push_back(Cand{variant, tpb, wpt, frac, 1e30f});
+        }
+      for (auto& cd : cands) {
+        st = time_cand(c, cd, 1, &cd.per);
+        if (st != LD_OK) { batch_free(b); return st; }
+      }
+      std::sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.per < y.per; });
+      const size_t top = std::min<size_t>(4, cands.size());
+      for (size_t i = 0; i < top; ++i) {
+        st = time_cand(c, cands[i], 3, &cands[i].per);
+        if (st != LD_OK) { batch_free(b); return st; }
+      }
+      std::sort(cands.begin(), cands.begin() + top, [](const Cand& x, const Cand& y) { return x.per < y.per; });
+      for (const auto& cd : cands)
+        if (c.tuned[cd.variant] == 0.f || cd.per * 1e9f < c.tuned[cd.variant]) c.tuned[cd.variant] = cd.per * 1e9f;
+      if (!cands.empty() && cands[0].per < best.per) { best = cands[0]; best_shift = shift; }
+    }
+    if (best_shift != c.kshift) {
+      st = apply_shift(c, best_shift);
       if (st != LD_OK) { batch_free(b); return st; }
     }
-    std::sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.per < y.per; });
-    const size_t top = std::min<size_t>(4, cands.size());
-    for (size_t i = 0; i < top; ++i) {
-      st = time_cand(c, cands[i], 3, &cands[i].per);
-      if (st != LD_OK) { batch_free(b); return st; }
-    }
-    std::sort(cands.begin(), cands.begin() + top, [](const Cand& x, const Cand& y) { return x.per < y.per; });
-    for (const auto& cd : cands)
-      if (c.tuned[cd.variant] == 0.f || cd.per * 1e9f < c.tuned[cd.variant]) c.tuned[cd.variant] = cd.per * 1e9f;
-    if (!cands.empty() && cands[0].per < 1e29f) {
-      c.wpt = cands[0].wpt; c.grid_frac = cands[0].frac; c.split = cands[0].variant == 1; c.tpb = cands[0].tpb;
+    if (best.per < 1e29f) {
+      c.wpt = best.wpt; c.grid_frac = best.frac; c.split = best.variant == 1; c.tpb = best.tpb;
     }
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[key] = std::make_tuple(c.wpt, c.grid_frac, c.split, c.tpb);
+    g_tune[key] = std::make_tuple(c.wpt, c.grid_frac, c.split, c.tpb, c.kshift);
   }
   st = build_queue();
   if (st != LD_OK) { batch_free(b); return st; }
@@ -531,8 +603,9 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
            b->hchunks.size(), (int)std::count_if(b->plans.begin(), b->plans.end(), [](ld_plan* q) { return q != nullptr; }));
   b->desc = buf;
   for (auto& c : b->classes) {
-    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, tpb=%d, grid=%d%s", c.D,
-             c.WB, c.WA, c.probs.size(), c.nchunks, c.wpt, c.tpb, class_grid(c), c.split ? ", column split" : "");
+    snprintf(buf, sizeof buf, "; D=%d int32=%d int8x4=%d: %zu matrices, %d chunks, wpt=%d, tpb=%d, k-%d, grid=%d%s",
+             c.D, c.WB, c.WA, c.probs.size(), c.nchunks, c.wpt, c.tpb, c.kshift, class_grid(c),
+             c.split ? ", column split" : "");
     b->desc += buf;
     if (c.tuned[0] > 0.f && c.tuned[1] > 0.f) {
       snprintf(buf, sizeof buf, " (tuned ms per 1e9 labelings: %.3f, split %.3f)", c.tuned[0], c.tuned[1]);
