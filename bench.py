@@ -760,6 +760,8 @@ def run_batch(args) -> None:
                 solved.append({"index": idx, "rows": m.shape[0], "cols": m.shape[1], "labelings": lab,
                                "value": sol.value, "gray_index": sol.gray_index, "kernel_ms": sol.kernel_ms,
                                "wall_s": time.perf_counter() - t0})
+                if args.tail_out:   # after every solve, so that a stopped run keeps what it solved
+                    Path(args.tail_out).write_text(json.dumps({"solved": solved}, indent=1))
             elif m.shape[0] > args.tail_rows:
                 rest.append({"index": idx, "rows": m.shape[0], "cols": m.shape[1], "labelings": lab})
         rate = (sum(x["labelings"] for x in solved) / max(1e-9, sum(x["kernel_ms"] for x in solved) * 1e-3)

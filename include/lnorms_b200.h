@@ -107,6 +107,11 @@ typedef struct {
     int32_t walk_fetch;         /* table kernel: 0 = warps fetch walks from a
                                    counter as they finish (balanced); -1 =
                                    every thread takes a fixed share         */
+    int32_t batch_row_search;   /* ld_batch_create with autotune: 1 = also try
+                                   one or two low rows fewer per int32 class
+                                   (measured: no faster replay on the 4096-
+                                   matrix batch, 4x the creation time); 0 = the
+                                   largest table that fits                   */
     void *stream;               /* cudaStream_t, NULL = the plan's own stream      */
 } ld_options;
 

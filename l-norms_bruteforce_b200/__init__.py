@@ -46,7 +46,7 @@ class Options(C.Structure):
                 ("lane_bits", C.c_int32), ("shard_index", C.c_int32), ("shard_count", C.c_int32),
                 ("prune_policy", C.c_int32), ("enumerate_all", C.c_int32), ("batch_split", C.c_int32),
                 ("column_split", C.c_int32), ("paired_walks", C.c_int32), ("pack16", C.c_int32),
-                ("walk_fetch", C.c_int32), ("stream", C.c_void_p)]
+                ("walk_fetch", C.c_int32), ("batch_row_search", C.c_int32), ("stream", C.c_void_p)]
 
 
 class ProblemInfo(C.Structure):

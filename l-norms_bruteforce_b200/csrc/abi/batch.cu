@@ -492,7 +492,8 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     for (int p : c.probs) mean += (double)walks[p];
     mean /= std::max<size_t>(1, c.probs.size());
     const auto key = std::make_tuple(c.D, c.WB, c.WA, (int)std::log2(std::max(1.0, mean)),
-                                     (int)o.batch_split * 1000 + (int)o.threads_per_block);
+                                     (int)o.batch_split * 1000 + (int)o.threads_per_block * 10 +
+                                         (o.batch_row_search > 0 ? 1 : 0));
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune.find(key);
@@ -514,7 +515,7 @@ extern "C" ld_status ld_batch_create(int32_t count, const int64_t* const* mats, 
     // low-row counts: the largest that fits (shift 0) and, for int32
     // classes, one or two rows fewer (smaller tables, more walks)
     int max_shift = 0;
-    if (c.WA == 0)
+    if (c.WA == 0 && o.batch_row_search > 0)
       for (int p : c.probs) max_shift = std::max(max_shift, std::min(2, kmax[p]));
     Cand best{0, c.tpb, c.wpt, c.grid_frac, 1e30f};
     int best_shift = 0;
