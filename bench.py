@@ -753,7 +753,10 @@ def run_batch(args) -> None:
     tail_out = None
     if tail:
         solved, rest = [], []
+        skip = {int(x) for x in args.tail_skip.split(",") if x.strip()}
         for idx, m, lab in sorted(tail, key=lambda x: x[2]):
+            if idx in skip:
+                continue
             if args.tail_min_rows <= m.shape[0] <= args.tail_rows:
                 t0 = time.perf_counter()
                 sol = ld.solve_reduced(m, 3, False, ld.options(device=local))
@@ -968,6 +971,8 @@ def main() -> None:
                     help="config 4: also solve the d = 3 tail matrices of at most this many rows, one by one")
     ap.add_argument("--tail-min-rows", type=int, default=0,
                     help="config 4: solve only the tail matrices with at least this many rows (a later part)")
+    ap.add_argument("--tail-skip", default="",
+                    help="config 4: comma-separated workload indices of tail matrices solved in an earlier part")
     ap.add_argument("--tail-out", default="", help="config 4: write the tail's per-matrix results to this JSON file")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="config 4: the first N of the 4096 matrices (0 = all; for small profiling runs)")
