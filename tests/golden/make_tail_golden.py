@@ -2,13 +2,14 @@
 workload's tail (the d = 3 matrices with more than 3^20 labelings, solved
 one by one outside the batch replay).
 
-    python tests/golden/make_tail_golden.py [count]
+    python tests/golden/make_tail_golden.py [count]      (27: every 22-row tail matrix)
 
 Regenerates the workload with its seeded generator, reduces each matrix
 with the library's preprocessing (no flag: the matrix as read), picks the
-`count` tail matrices with the fewest labelings (22 rows, 3^21 labelings
-each) and enumerates them with the oracle (oracle/lnorm_oracle.c, all host
-threads; about a minute each).  Writes tests/golden/config4_tail.json,
+`count` tail matrices with the fewest labelings (the 27 of 22 rows have
+3^21 labelings each) and enumerates them with the oracle
+(oracle/lnorm_oracle.c, all host threads; one to three minutes each on 8
+cores).  Writes tests/golden/config4_tail.json,
 which tests/test_gpu_batch.py compares the GPU's single solves with."""
 import json
 import os
@@ -22,7 +23,7 @@ sys.path.insert(0, str(ROOT))
 
 
 def main():
-    count = int(sys.argv[1]) if len(sys.argv) > 1 else 3
+    count = int(sys.argv[1]) if len(sys.argv) > 1 else 27
     from conftest import load_package
     import oracle_ffi as O
     ld = load_package()

@@ -139,14 +139,14 @@ def test_batch_column_split(ld, split):
 def test_config4_tail_matches_oracle(ld, workloads):
     """The d = 3 tail of the 4096-matrix workload (more than 3^20 labelings
     each, solved one by one outside the batch replay): its smallest
-    matrices, 22 rows (3^21 labelings), against values the oracle computed
-    on the CPU (tests/golden/make_tail_golden.py; about a minute each
-    there, some 20-30 ms here)."""
+    matrices, all 27 of 22 rows (3^21 labelings), against values the
+    oracle computed on the CPU (tests/golden/make_tail_golden.py; one to
+    three minutes each there, 20-45 ms each here)."""
     import json
     from pathlib import Path
     gold = json.loads((Path(__file__).parent / "golden" / "config4_tail.json").read_text())
     insts = workloads.config4()
-    assert len(gold) >= 3
+    assert len(gold) == 27
     for g in gold:
         p = ld.Problem.from_matrix(insts[g["index"]].matrix, insts[g["index"]].d)
         red = p.reduced
